@@ -123,6 +123,47 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 # algorithmic bytes per stage (one launch covering `nr` RHS)
 # ---------------------------------------------------------------------------
+# kernel behind each profiled stage of a 16-RHS product (K = 256: the
+# tensor-core spread takes calls of >= 8 RHS)
+STAGE_KERNEL = {"gather_forces": "k_gather_forces + k_gather_forces_rs", "real_space": "k_pair_apply<16>",
+                "spread_tc": "k_spread_tc<K>", "spread_xfwd": "k_spread_xfwd<K>",
+                "yfft_fwd": "k_ypass_tma<K,fwd>", "zfft_influence": "k_zpass_fused_tma<K>",
+                "yfft_inv": "k_ypass_tma<K,inv>", "xinv_interp": "k_xinv_interp<K>", "combine": "k_combine"}
+
+
+def rename_stages(stages: dict, K: int, nr: int) -> dict:
+    """The library's stage 'spread_x' is the tensor-core spread for K = 256
+    and >= 8 RHS, the shared-memory spread + x FFT otherwise."""
+    tc = K == 256 and nr >= 8 and os.environ.get("STOKESDT_NO_TC", "0") != "1"
+    return {("spread_tc" if tc else "spread_xfwd") if k == "spread_x" else k: v for k, v in stages.items()}
+
+
+def cufft_reference_ms(K: int, ngrids: int, dev, reps: int = 3):
+    """cuFFT (torch.fft) r2c and c2r of `ngrids` K^3 FP32 grids on the
+    current stream: the library FFT the hand-written passes stand beside
+    (timing reference only; cuFFT is not on the product path)."""
+    import torch
+    x = torch.randn((ngrids, K, K, K), dtype=torch.float32, device=dev)
+    out = {}
+    X = torch.fft.rfftn(x, dim=(1, 2, 3))          # warm-up (plan creation)
+    torch.fft.irfftn(X, s=(K, K, K), dim=(1, 2, 3))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize(dev)
+    ev[0].record()
+    for _ in range(reps):
+        X = torch.fft.rfftn(x, dim=(1, 2, 3))
+    ev[1].record()
+    for _ in range(reps):
+        y = torch.fft.irfftn(X, s=(K, K, K), dim=(1, 2, 3))
+    ev[2].record()
+    torch.cuda.synchronize(dev)
+    out["r2c_ms"] = round(ev[0].elapsed_time(ev[1]) / reps, 4)
+    out["c2r_ms"] = round(ev[1].elapsed_time(ev[2]) / reps, 4)
+    del x, X, y
+    torch.cuda.empty_cache()
+    return out
+
+
 def stage_bytes(stage: str, N: int, K: int, p: int, nr: int, pairs: int = 0) -> float:
     """Bytes a stage must move at minimum, per launch of nr RHS.  Ghat1 is one
     component's complex half-spectrum K*K*(K/2+1)*8 B; the real-space grid
@@ -132,7 +173,7 @@ def stage_bytes(stage: str, N: int, K: int, p: int, nr: int, pairs: int = 0) -> 
     float4 force rows once and writes the FP32 result."""
     g1 = K * K * (K // 2 + 1) * 8.0
     part = N * (4 + 3 * p * 4.0)            # packed base index + spline weights
-    if stage == "spread_xfwd":
+    if stage in ("spread_xfwd", "spread_tc"):
         return 3 * nr * g1 + part + 3 * nr * N * 4.0
     if stage in ("yfft_fwd", "yfft_inv"):
         return 2 * 3 * nr * g1
@@ -380,7 +421,7 @@ def run_b200(args):
 
     # per-stage profile and roofline of the dominant kernel
     log(f"M.f 16 RHS: {mf_ms / reps:.3f} ms")
-    stages = mob.profile(INTERVAL, 3)
+    stages = rename_stages(mob.profile(INTERVAL, 3), K, INTERVAL)
     log(f"stages: {stages}")
     dom = max((k for k in stages if k != "combine"), key=lambda k: stages[k])
     peaks, peak_kind = measured_peaks()
@@ -396,7 +437,8 @@ def run_b200(args):
             traffic = tj[dom]["bytes_per_launch_at_bench_size"]
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                "kernel": dom, "peak_source": peak_kind,
+                "kernel": STAGE_KERNEL.get(dom, dom).replace("<K>", f"<{K}>"), "stage": dom,
+                "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": algo, "launch_ms": round(stages[dom], 4)}
     # the whole 16-RHS product against the unfused per-RHS figure 4G + 4Ghat + T
     # (real grid G = 3 K^3 4 B, half spectrum Ghat = 3 K^2 (K/2+1) 8 B, table
@@ -406,6 +448,21 @@ def run_b200(args):
     roofline_mf = {"bound": "hbm", "achieved": round(mf_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                    "frac": round(mf_gbs / peaks["hbm_gbs"], 4), "peak_source": peak_kind,
                    "unfused_bytes_per_rhs": unfused, "product_ms": round(mf_ms / reps, 4)}
+
+    # cuFFT beside the hand-written chain: r2c + c2r of the 3 x 16 grids of
+    # one 16-RHS product (the chain's transforms are fused with the spread,
+    # the influence multiply and the interpolation)
+    cufft = None
+    try:
+        cufft = cufft_reference_ms(K, 3 * INTERVAL, dev)
+        chain = ("spread_tc", "spread_xfwd", "yfft_fwd", "zfft_influence", "yfft_inv", "xinv_interp")
+        cufft["ngrids"] = 3 * INTERVAL
+        cufft["hand_written_chain_ms"] = round(sum(stages.get(k, 0.0) for k in chain), 4)
+        cufft["note"] = ("hand_written_chain_ms includes the spread, the influence multiply and the "
+                         "interpolation fused into the transforms; cuFFT's r2c + c2r are transforms only")
+        log(f"cuFFT reference: {cufft}")
+    except Exception as exc:  # noqa: BLE001 (timing reference only)
+        log(f"cuFFT reference skipped: {exc}")
 
     # end to end through the host-pointer C ABI (pinned host buffers)
     e2e = None
@@ -463,6 +520,7 @@ def run_b200(args):
                            "p99": round(float(np.percentile(lat, 99)), 3)},
             "lanczos_iters": iters_seen[-args.steps:],
             "stage_ms_16rhs": {k: round(v, 4) for k, v in stages.items()},
+            "cufft_reference": cufft,
         }
         print(json.dumps(out))
     if dist is not None:

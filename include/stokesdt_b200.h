@@ -3,8 +3,8 @@
  * Brownian path.  Plain C types only: opaque handles, pointers and sizes.
  *
  * Each entry point replaces a reference interface (paths relative to the
- * StokesDT project; see INTEGRATION.md for the C++ adapters that put these
- * behind MobBase / BrwnBase):
+ * StokesDT project; the C++ adapters in stokesdt_b200_adapters.hpp put these
+ * behind MobBase / BrwnBase / ForceBase):
  *
  *   sdt_spme_create        MobSpme::MobSpme + MobSpme::Init   src/mob/mob_spme.h:27-39,
  *                          src/mob/mob_spme.cc:19-132; engine CreateSpmeEngine
@@ -103,7 +103,10 @@ int sdt_spme_mulvec_device(sdt_spme *h, int mode, int nrhs, double alpha, int ld
  * otherwise).  Device pointers, asynchronous on the engine stream.  All calls
  * on a device share that array: calls that overlap on the GPU race.  The
  * first call on a device looks up the array's address (make it before any
- * stream capture). */
+ * stream capture), and so does the first call after cudaDeviceReset.  It
+ * always walks the cell list, also on an engine that stores a pair list, so
+ * it is slower than the allocating real-space product there.  In place
+ * (d_f == d_v) is allowed with ldf == ldv. */
 int sdt_spme_real_mulvec_noalloc(sdt_spme *h, int nrhs, double alpha, int ldf, const double *d_f,
                                  double beta, int ldv, double *d_v);
 
@@ -351,6 +354,16 @@ const char *sdt_version(void);
  * milliseconds of each stage to stage_ms[0..n).  Returns n (the number of
  * stages, <= max_stages) or a negative sdt_status. */
 int sdt_spme_profile_mulvec(sdt_spme *h, int nrhs, int reps, double *stage_ms, int max_stages);
+
+/* Forward transform of the spread forces, for checking the hand-written FFT
+ * against an independent one: for nrhs (1..16) force vectors (device
+ * pointer, leading dimension ldf >= 3*npos) writes the half spectra
+ * spec[r][c][kz][ky][kx], kx = 0..K/2, of the spread grids (the grid the
+ * reference spreads in src/mob/spme.cc:313-363 and transforms with its
+ * forward DFTI call, src/mob/spme.cc:754-756) as interleaved FP32 (re, im)
+ * pairs: nrhs * 3 * K * K * (K/2 + 1) * 2 floats.  Monodisperse engines, grid
+ * dimension <= 256.  Asynchronous on the engine stream. */
+int sdt_spme_spectrum_device(sdt_spme *h, int nrhs, int ldf, const double *d_f, float *d_spec);
 
 /* Name of profile stage i ("" when out of range). */
 const char *sdt_profile_stage_name(int stage);

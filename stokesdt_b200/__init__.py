@@ -129,6 +129,7 @@ SIGNATURES = {
     "sdt_lanczos_set_stream": (ctypes.c_int, [_vp, _vp]),
     "sdt_spme_profile_mulvec": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]),
     "sdt_profile_stage_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "sdt_spme_spectrum_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "sdt_kernel_launches": (ctypes.c_ulonglong, []),
     "sdt_lanczos_history": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "sdt_lanczos_products": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
@@ -263,6 +264,13 @@ class MobSpme:
         if n < 0:
             self._check(n)
         return {lib().sdt_profile_stage_name(i).decode(): out[i] for i in range(n)}
+
+    def spectrum_device(self, num_rhs, ldf, d_f: int, d_spec: int):
+        """Half spectra of the spread forces (forward transform only), written
+        to d_spec as complex64 [num_rhs][3][K][K][K/2+1]; a diagnostic for
+        checking the hand-written FFT against an independent one."""
+        self._need()
+        self._check(lib().sdt_spme_spectrum_device(self._h, int(num_rhs), int(ldf), _vp(d_f), _vp(d_spec)))
 
     def set_pairlist(self, enable: bool):
         """Store the real-space pairs at every Update (default) or walk the

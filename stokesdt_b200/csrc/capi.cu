@@ -626,9 +626,17 @@ int sdt_spme_profile_mulvec(sdt_spme *h, int nrhs, int reps, double *stage_ms, i
     return st == SDT_OK ? sdt::kNumStages : st;
 }
 
+int sdt_spme_spectrum_device(sdt_spme *h, int nrhs, int ldf, const double *d_f, float *d_spec)
+{
+    if (!h || !d_f || !d_spec) return SDT_ERR_INVALID;
+    sdt::SpmeEngine *e = &h->e;
+    CAPI_CUDA(e, cudaSetDevice(e->device));
+    return sdt::spme_spectrum(e, nrhs, ldf, d_f, d_spec);
+}
+
 const char *sdt_profile_stage_name(int stage)
 {
-    static const char *names[sdt::kNumStages] = {"gather_forces", "real_space", "spread_xfwd", "yfft_fwd",
+    static const char *names[sdt::kNumStages] = {"gather_forces", "real_space", "spread_x", "yfft_fwd",
                                                  "zfft_influence", "yfft_inv", "xinv_interp", "combine"};
     return (stage >= 0 && stage < sdt::kNumStages) ? names[stage] : "";
 }

@@ -140,18 +140,18 @@ struct SpmeEngine {
     // (K <= 256, TMA path; cleared by STOKESDT_NO_ZFUSE=1)
     bool zfused = true;
     // tensor-core spread (K = 256, calls of >= kTcRhsPerCta RHS; cleared by
-    // STOKESDT_NO_TC=1, and for batch and served engines): per row block the
-    // particles whose support reaches it (padded to whole 32-particle
-    // chunks), their 32 row weights wz*wy and their x-transformed weight
+    // STOKESDT_NO_TC=1, and for batch and served engines): per 2x2 row block
+    // the particles whose support reaches it (padded to whole 16-particle
+    // chunks), their 4 row weights wz*wy and their x-transformed weight
     // rows as TF32 hi/lo MMA operand tiles, rebuilt at every update
     bool tc_enabled = true;
     bool tc_ready = false;
     long long tc_cap = 0;          // entries the arrays hold
     int *d_tc_cnt = nullptr;       // [nblk] counts, then cursors
-    int *d_tc_start = nullptr;     // [nblk + 1] entry starts (multiples of 32)
+    int *d_tc_start = nullptr;     // [nblk + 1] entry starts (multiples of 16)
     int *d_tc_slot = nullptr;      // [entries] spread-order slot, -1 for padding
-    float *d_tc_w = nullptr;       // [entries][32] row weights
-    float *d_tc_bx = nullptr;      // [chunks][2][K][32] operand tiles
+    float *d_tc_w = nullptr;       // [entries][4] row weights
+    float *d_tc_bx = nullptr;      // [chunks][2][K][16] operand tiles
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
@@ -179,6 +179,8 @@ int spme_mulvec(SpmeEngine *e, int mode, int nrhs, double alpha, int ldf, const 
 void spme_free(SpmeEngine *e);
 int spme_reserve(SpmeEngine *e, int rhs);
 int spme_profile(SpmeEngine *e, int nrhs, int reps, double *stage_ms);
+// Forward transform of the spread forces (diagnostic; see spme.cu).
+int spme_spectrum(SpmeEngine *e, int nrhs, int ldf, const double *d_f, float *d_spec);
 
 // real_space.cu: adds the matrix-free real-space sum (without the self term)
 // of `rb` RHS to d_vreal ([rb][3N], zeroed by the caller).

@@ -22,7 +22,17 @@
 //     RHS and component) before reading it;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress, once per device with that device current; make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The address is kept with
+//     the CUDA context it belongs to: after cudaDeviceReset (a new primary
+//     context) the next call looks it up again, so that call too must come
+//     before any stream capture;
+//   - the product always walks the cell list on the fly, also when the engine
+//     holds a stored real-space pair list (the stored-list product needs a
+//     larger force layout than the fixed array is sized for), so it runs
+//     slower than sdt_spme_mulvec_device(SDT_MOB_REAL) on such an engine;
+//   - d_f == d_v (in place) is allowed when ldf == ldv.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "../../include/stokesdt_b200.h"
@@ -40,19 +50,43 @@ static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
 
 static std::mutex g_noalloc_mutex;
 static float *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+static CUcontext g_noalloc_ctx[kNoAllocMaxDevices] = {};
 
-// Device address of the scratch array on `device` (current device).
+// The CUDA context current on this thread (driver entry point, so the library
+// needs no link-time dependency on libcuda).
+static CUcontext current_context()
+{
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<Fn>(p);
+        cudaGetLastError();
+        return static_cast<Fn>(nullptr);
+    }();
+    CUcontext ctx = nullptr;
+    if (fn && fn(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+    return ctx;
+}
+
+// Device address of the scratch array on `device` (current device), looked
+// up again when the context has changed since the last lookup.
 static int noalloc_scratch(int device, float **out)
 {
     if (device < 0 || device >= kNoAllocMaxDevices) return kErrInvalid;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
+    const CUcontext ctx = current_context();
+    if (!g_noalloc_ptr[device] || !ctx || ctx != g_noalloc_ctx[device]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
+            g_noalloc_ptr[device] = nullptr;
             return kErrCuda;
         }
         g_noalloc_ptr[device] = static_cast<float *>(p);
+        g_noalloc_ctx[device] = ctx;
     }
     *out = g_noalloc_ptr[device];
     return kOk;
@@ -72,10 +106,11 @@ __global__ void k_noalloc_gather(int n, int nr, const double *__restrict__ f, in
 }
 
 // v := alpha * (real + self * f) + beta * v in FP64 (beta == 0 ignores v).
-__global__ void k_noalloc_combine(int n3, int nr, double alpha, double beta,
-                                  const double *__restrict__ f, int ldf,
+// f and v may be the same array (ldf == ldv): each element is read and then
+// written by one thread only, so they are not declared __restrict__.
+__global__ void k_noalloc_combine(int n3, int nr, double alpha, double beta, const double *f, int ldf,
                                   const double *__restrict__ self, const float *__restrict__ vreal,
-                                  double *__restrict__ v, int ldv)
+                                  double *v, int ldv)
 {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (idx >= (long long)n3 * nr) return;

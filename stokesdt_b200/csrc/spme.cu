@@ -977,7 +977,10 @@ __global__ void k_combine(int n3, int nr, int mode, double alpha, double beta, d
 template <int K>
 __host__ __device__ constexpr int kZFusedThreads() { return kTileZF * FftShape<K>::N2; }
 
-template <int K>
+// FWD_ONLY stops after the forward z transform and stores the spectrum (the
+// forward-transform diagnostic sdt_spme_spectrum_device); the product uses
+// FWD_ONLY = false.
+template <int K, bool FWD_ONLY = false>
 __global__ void __launch_bounds__(kZFusedThreads<K>(), 6)
 k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap tabmap,
                   const float2 *__restrict__ tw, const float *__restrict__ kmap, int *err, int r0)
@@ -1044,6 +1047,27 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
             for (int j = 0; j < N2; j++) b[c][rr][j] = at(c, k1 * N2 + ((j + k1) & (N2 - 1)));
             dft_reg<N2, false>(b[c][rr]);
         }
+    if constexpr (FWD_ONLY) {
+        __syncthreads();  // every thread is done reading the transposed data
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int rr = 0; rr < NR; rr++)
+                static_for<N2>([&](auto kc) {
+                    constexpr int k2 = decltype(kc)::value;
+                    at(c, t + rr * N2 + N1 * k2) = b[c][rr][SlotOf<N2, k2>::value];
+                });
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            for (int c2 = 0; c2 < 3; c2++)
+                for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
+                    tma_store_4d(&map, sm + c2 * CS + z0 * kTileZF, kx0, y, z0, 3 * r + c2);
+            bulk_commit();
+            bulk_wait_read_all();
+        }
+        return;
+    }
     // influence: Ghat <- m2(k) (I - k k^T / k^2) Ghat, zero at k = 0
     const int kx = kx0 + col;
     const float fkx = kx <= H ? __ldg(&kmap[kx]) : 0.0f;
@@ -1134,9 +1158,11 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
 
 static inline int grid1d(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// fwd_only: stop after the forward transform (spread + x, y and z FFTs),
+// leaving the half spectrum in d_cgrid (fused z pass only).
 template <int K>
 static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *iscale, int r0 = 0,
-                      cudaStream_t st = nullptr)
+                      cudaStream_t st = nullptr, bool fwd_only = false)
 {
     constexpr int H = K / 2;
     cudaStream_t s = st ? st : e->stream;
@@ -1159,10 +1185,16 @@ static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *isc
         SDT_CUDA(cudaFuncSetAttribute(k_ypass_tma<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
         SDT_CUDA(cudaFuncSetAttribute(k_zpass_influence_tma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smz_tma));
-        if constexpr (K <= 256)
+        if constexpr (K <= 256) {
             SDT_CUDA(cudaFuncSetAttribute(k_zpass_fused_tma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smzf_tma));
+            if (fwd_only)
+                SDT_CUDA(cudaFuncSetAttribute(k_zpass_fused_tma<K, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smzf_tma));
+        }
     }
+    if (fwd_only && !(K <= 256 && e->tma_ready && e->zfused))
+        return set_error(e, kErrUnsupported, "the forward-spectrum diagnostic needs the fused z pass (K <= 256)");
     const int ty = kTileX * FftShape<K>::N2;
     const int tz = 3 * kTileZ * FftShape<K>::N2;
     if (K == 256 && e->tc_ready && nr >= kTcRhsPerCta) {
@@ -1184,6 +1216,12 @@ static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *isc
         if constexpr (K <= 256) {
             if (e->zfused) {
                 const CUtensorMap &tabmapf = tab == e->d_tab2 ? e->tmap_tab2f : e->tmap_tab0f;
+                if (fwd_only) {
+                    k_zpass_fused_tma<K, true><<<dim3(nr, ntilezf, K), kZFusedThreads<K>(), smzf_tma, s>>>(
+                        e->tmap_zf, tabmapf, e->d_tw_full, e->d_kmap, e->d_err, r0);
+                    SDT_LAUNCH_CHECK();
+                    return kOk;
+                }
                 k_zpass_fused_tma<K><<<dim3(nr, ntilezf, K), kZFusedThreads<K>(), smzf_tma, s>>>(
                     e->tmap_zf, tabmapf, e->d_tw_full, e->d_kmap, e->d_err, r0);
                 fused = true;
@@ -1219,14 +1257,14 @@ static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *isc
 }
 
 static int recip_dispatch(SpmeEngine *e, int nr, const float *tab, const double *iscale, int r0 = 0,
-                          cudaStream_t st = nullptr)
+                          cudaStream_t st = nullptr, bool fwd_only = false)
 {
     switch (e->K) {
-        case 32: return recip_pass<32>(e, nr, tab, iscale, r0, st);
-        case 64: return recip_pass<64>(e, nr, tab, iscale, r0, st);
-        case 128: return recip_pass<128>(e, nr, tab, iscale, r0, st);
-        case 256: return recip_pass<256>(e, nr, tab, iscale, r0, st);
-        case 512: return recip_pass<512>(e, nr, tab, iscale, r0, st);
+        case 32: return recip_pass<32>(e, nr, tab, iscale, r0, st, fwd_only);
+        case 64: return recip_pass<64>(e, nr, tab, iscale, r0, st, fwd_only);
+        case 128: return recip_pass<128>(e, nr, tab, iscale, r0, st, fwd_only);
+        case 256: return recip_pass<256>(e, nr, tab, iscale, r0, st, fwd_only);
+        case 512: return recip_pass<512>(e, nr, tab, iscale, r0, st, fwd_only);
         default: return set_error(e, kErrUnsupported, "grid dimension must be 32, 64, 128, 256 or 512");
     }
 }
@@ -1613,6 +1651,30 @@ int spme_mulvec(SpmeEngine *e, int mode, int nrhs, double alpha, int ldf, const 
         SDT_LAUNCH_CHECK();
         prof_mark(e, kStCombine);
     }
+    return kOk;
+}
+
+// Forward transform of the spread forces of nrhs (<= 16) RHS: the half
+// spectra Ghat[r][c][kz][ky][kx], kx <= K/2, as complex FP32 pairs (no
+// counterpart in the reference; checks the hand-written FFT against an
+// independent one).  Monodisperse engines with the fused z pass only.
+int spme_spectrum(SpmeEngine *e, int nrhs, int ldf, const double *d_f, float *d_spec)
+{
+    if (!e->updated) return set_error(e, kErrState, "Update() must be called first");
+    if (!e->mono) return set_error(e, kErrUnsupported, "spectrum diagnostic: monodisperse engines only");
+    if (nrhs <= 0 || nrhs > e->rhs_chunk_max) return set_error(e, kErrInvalid, "spectrum: 1 <= nrhs <= 16");
+    const int n = e->npos, K = e->K, H1 = e->K / 2 + 1;
+    if (ldf < 3 * n) return set_error(e, kErrInvalid, "ldf must be >= 3*npos");
+    int st = spme_reserve(e, nrhs);
+    if (st != kOk) return st;
+    k_gather_forces<<<grid1d((long long)n * nrhs, 256), 256, 0, e->stream>>>(n, nrhs, d_f, ldf, e->d_sp_perm,
+                                                                           nullptr, e->d_fs_sp);
+    SDT_LAUNCH_CHECK();
+    st = recip_dispatch(e, nrhs, e->d_tab0, nullptr, 0, nullptr, true);
+    if (st != kOk) return st;
+    SDT_CUDA(cudaMemcpy2DAsync(d_spec, (size_t)H1 * sizeof(float2), e->d_cgrid, (size_t)e->XS * sizeof(float2),
+                               (size_t)H1 * sizeof(float2), (size_t)nrhs * 3 * K * K, cudaMemcpyDeviceToDevice,
+                               e->stream));
     return kOk;
 }
 

@@ -9,14 +9,14 @@
 // Re Bx(0..H), Im Bx(1..H-1) of a particle form one GEMM column; with M =
 // those 256 values (two 128-row MMA tiles), N = 8 RHS x 3 components x 4
 // rows = 96
-// and K = the block's particles in chunks of 32, tcgen05.mma (kind::tf32,
+// and K = the block's particles in chunks of 16, tcgen05.mma (kind::tf32,
 // FP32 accumulation in tensor memory) computes the block's half spectra
 // directly: no shared-memory atomics and no x FFT.  FP32 accuracy comes from
 // the 3-term TF32 split a*b ~ ah*bh + ah*bl + al*bh (relative error ~1e-7 on
 // the spectra, like the FP32 FFT path).
 //
 // Per Update (tc_build): per-block particle lists padded to whole chunks,
-// each entry's 32 row weights wz*wy, and each chunk's Bx operand tile (hi and
+// each entry's 4 row weights wz*wy, and each chunk's Bx operand tile (hi and
 // lo TF32 parts) already in the K-major core-matrix layout of the MMA, so a
 // CTA stages a chunk with two bulk copies.
 #include <algorithm>

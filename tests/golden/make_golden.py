@@ -21,10 +21,14 @@ Cases (reference test that each one follows):
                       system: RSA N=2000 phi=0.3, jittered
   bd_cfg3_traj        config 3 (N=2e4, phi=0.3, K=128, steric): the first 10 BD steps composed
                       from the reference's MobSpme, BrwnLanczos and StericForce (--bd only)
+  bd_cfg3_traj_tight  the same with Lanczos tol 1e-8, max_iters 200 (--bd-tight only)
   lanczos_cfg2_proj   config 2 at full size (N=1e5, K=256, p=6, xi=0.35): BrwnLanczos
                       (tol 1e-6, max_iters 100, 16 RHS) on the reference's MobSpme;
                       the iteration count and 64 random projections of the first two
                       Brownian vectors (--cfg2 only: ~15 minutes on 8 cores)
+  mf_cfg2_proj        config 2 at full size: MobSpme MulVector / RealMulVector /
+                      RecipMulVector on 4 RHS (alpha 1.3, beta 0.7); 64 random projections,
+                      norms and the first 512 particles' outputs per mode (--mf-cfg2 only)
 Random inputs come from numpy's PCG64 with fixed seeds (the reference's MKL
 VSL stream cannot be reproduced here).
 """
@@ -126,7 +130,7 @@ def steric_cases(refdir):
     steric_case("steric_cfg3", pos, np.ones(N), L, 2.0, 125.0, 23)
 
 
-def bd_cfg3_case(name, nsteps=10):
+def bd_cfg3_case(name, nsteps=10, tol=None, max_iters=None):
     """Config 3, first `nsteps` steps of BDSimBox::Advance
     (src/simbox/simbox_bd.cc:296-366) composed from the reference's own
     MobSpme, BrwnLanczos (1 RHS per step, tol 1e-5) and StericForce, FP64,
@@ -142,7 +146,8 @@ def bd_cfg3_case(name, nsteps=10):
     rdi = np.ones(N)
     pos0 = wl.rsa_positions(N, L, w.seed_pos).reshape(-1)
     sp = ref.RefMob.spme(rdi, L, w.xi, w.rmax, w.dim, w.porder)
-    lz = ref.RefLanczos(n3, w.max_iters, 1, w.lanczos_tol)
+    tol = w.lanczos_tol if tol is None else tol
+    lz = ref.RefLanczos(n3, max_iters or w.max_iters, 1, tol)
     st = ref.RefSteric(rdi, L, w.steric_r0, w.steric_k0)
     P = cfg2_projector(n3, seed=CFG2_PROJ_SEED + 3)
     pos = pos0.copy()
@@ -162,7 +167,7 @@ def bd_cfg3_case(name, nsteps=10):
         print(f"{name}: step {k + 1}, |pos - pos0| {norms[-1]:.6f}, Lanczos iterations {its[0]}")
     np.savez_compressed(os.path.join(HERE, name + ".npz"), proj=np.array(proj), norms=np.array(norms),
                         iters=np.array(iters), seed_proj=np.array(CFG2_PROJ_SEED + 3),
-                        nsteps=np.array(nsteps))
+                        nsteps=np.array(nsteps), tol=np.array(tol))
 
 
 CFG2_PROJ_SEED, CFG2_NPROJ = 2024, 64
@@ -206,22 +211,70 @@ def lanczos_cfg2_case(name):
                         seed_proj=np.array(CFG2_PROJ_SEED))
 
 
+MF_CFG2_NRHS, MF_CFG2_HEAD = 4, 512
+MF_CFG2_ALPHA, MF_CFG2_BETA = 1.3, 0.7
+
+
+def mf_cfg2_inputs(n3):
+    """Forces F (4 x 3N) and the initial v (4 x 3N, scaled by beta) of the
+    config-2 mobility-product fixture, seeded."""
+    rng = np.random.default_rng(9012)
+    return rng.standard_normal((MF_CFG2_NRHS, n3)), rng.standard_normal((MF_CFG2_NRHS, n3))
+
+
+def mf_cfg2_case(name):
+    """Config 2 at full size (N=1e5, phi=0.2, K=256, p=6, xi=0.35, rmax from
+    the tol-1e-6 rule): the reference's MobSpme MulVector (mode 0),
+    RealMulVector (1) and RecipMulVector (2) (src/mob/mob_spme.cc:219-263,
+    src/mob/spme.cc:714-839) on 4 RHS with alpha 1.3, beta 0.7.  Stores per
+    mode 64 fixed random projections of every output vector, their norms and
+    the outputs of the first 512 particles in full (~4 minutes on 8 cores)."""
+    from stokesdt_b200 import workloads as wl
+    w = wl.WORKLOADS["cfg2"]
+    N, n3 = w.npos, 3 * w.npos
+    pos = wl.rsa_positions(N, w.box, w.seed_pos)
+    rdi = np.ones(N)
+    F, V0 = mf_cfg2_inputs(n3)
+    sp = ref.RefMob.spme(rdi, w.box, w.xi, w.rmax, w.dim, w.porder)
+    sp.update(pos, rdi)
+    P = cfg2_projector(n3, seed=CFG2_PROJ_SEED + 7).astype(np.float64)
+    out = {}
+    for mode in (0, 1, 2):
+        v = sp.mulvec(F, MF_CFG2_ALPHA, MF_CFG2_BETA, V0.copy(), mode=mode)
+        out[f"proj{mode}"] = (P @ v.T).T
+        out[f"norms{mode}"] = np.linalg.norm(v, axis=1)
+        out[f"head{mode}"] = v[:, :3 * MF_CFG2_HEAD].copy()
+        print(f"{name}: mode {mode}, |v| {out[f'norms{mode}']}")
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), seed_proj=np.array(CFG2_PROJ_SEED + 7),
+                        alpha=np.array(MF_CFG2_ALPHA), beta=np.array(MF_CFG2_BETA),
+                        head=np.array(MF_CFG2_HEAD), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--cfg2", action="store_true", help="only the config-2 Lanczos fixture")
+    ap.add_argument("--mf-cfg2", action="store_true", help="only the config-2 mobility-product fixture")
     ap.add_argument("--lanczos", action="store_true", help="only the N1000 Lanczos fixture")
     ap.add_argument("--steric", action="store_true", help="only the steric-force fixtures")
     ap.add_argument("--bd", action="store_true", help="only the config-3 trajectory fixture")
+    ap.add_argument("--bd-tight", action="store_true",
+                    help="only the config-3 trajectory fixture at Lanczos tol 1e-8")
     a = ap.parse_args()
     if a.bd:
         bd_cfg3_case("bd_cfg3_traj")
+        return
+    if a.bd_tight:
+        bd_cfg3_case("bd_cfg3_traj_tight", tol=1e-8, max_iters=200)
         return
     if a.steric:
         steric_cases(a.ref)
         return
     if a.cfg2:
         lanczos_cfg2_case("lanczos_cfg2_proj")
+        return
+    if a.mf_cfg2:
+        mf_cfg2_case("mf_cfg2_proj")
         return
     if a.lanczos:
         pos, rdi, L = ref.parse_xyz(os.path.join(a.ref, "tests", "data", "N1000_Phi0.1.xyz"))

@@ -34,6 +34,7 @@ int main()
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src", "mob")), reason="reference tree absent")
 def test_adapters_compile_link_and_run_against_reference_headers():
     import stokesdt_b200 as sdt
+    import adapter_build
     sdt.lib()
     with tempfile.TemporaryDirectory() as d:
         src = os.path.join(d, "tu.cc")
@@ -41,15 +42,19 @@ def test_adapters_compile_link_and_run_against_reference_headers():
         with open(src, "w") as fh:
             fh.write(TU)
         # MobBase/BrwnBase constructors and destructors live in the reference's .cc files
-        extra = [os.path.join(REF, "src", "mob", "mob_base.cc"), os.path.join(REF, "src", "brwn", "brwn_base.cc"),
-                 os.path.join(REF, "src", "force", "force_base.cc")]
-        cmd = ["g++", "-std=gnu++98", "-D__declspec(a)=__attribute__((aligned(64)))",
-               "-I", os.path.join(ROOT, "include"), "-I", os.path.join(REF, "src", "mob"),
-               "-I", os.path.join(REF, "src", "brwn"), "-I", os.path.join(REF, "src", "util"),
-               "-I", os.path.join(REF, "src", "force"),
-               src] + extra + ["-o", exe, "-L", os.path.join(ROOT, "stokesdt_b200"),
-                               "-l:libstokesdt_b200.so",
-                               "-Wl,-rpath," + os.path.join(ROOT, "stokesdt_b200")]
+        cmd = adapter_build.compile_cmd(REF, src, exe)
+        cmd[-1] = "-Wl,-rpath," + os.path.join(ROOT, "stokesdt_b200")
         res = subprocess.run(cmd, capture_output=True, text=True)
         assert res.returncode == 0, res.stderr
         assert subprocess.run([exe]).returncode == 0
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src", "mob")), reason="reference tree absent")
+def test_adapter_parity_program_builds():
+    """The program the GPU adapter test runs (tests/adapter_parity.cc), built
+    against the reference headers into tests/_bin/ (it travels prebuilt)."""
+    import stokesdt_b200 as sdt
+    import adapter_build
+    sdt.lib()
+    exe = adapter_build.build(REF)
+    assert os.access(exe, os.X_OK)

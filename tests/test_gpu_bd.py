@@ -110,16 +110,28 @@ def test_config3_first_ten_steps_vs_reference_trajectory(gpu_available):
     BrwnLanczos and StericForce produce from the same random vectors
     (tests/golden/bd_cfg3_traj.npz: 64 projections of pos(k) - pos(0)).
     Both Lanczos runs stop at tol 1e-5, so the bar is 1e-4 relative per step."""
+    _config3_vs_reference("bd_cfg3_traj", None, None, 1e-4)
+
+
+def test_config3_first_ten_steps_tight_tolerance(gpu_available):
+    """The same trajectory with both Lanczos runs at tol 1e-8 (max_iters 200;
+    tests/golden/bd_cfg3_traj_tight.npz): the iterates are converged far
+    below the sqrt(M) z bar, so the trajectory is held to 1e-5 relative per
+    step."""
+    _config3_vs_reference("bd_cfg3_traj_tight", 1e-8, 200, 1e-5)
+
+
+def _config3_vs_reference(name, tol, max_iters, bar):
     import stokesdt_b200 as sdt
     from stokesdt_b200 import workloads as wl
     from conftest import golden
-    g = golden("bd_cfg3_traj")
+    g = golden(name)
     w = wl.WORKLOADS["cfg3"]
     N, n3 = w.npos, 3 * w.npos
     pos0 = wl.rsa_positions(N, w.box, w.seed_pos).reshape(-1)
     m = sdt.MobSpme(N, np.ones(N), w.box, w.xi, w.rmax, w.dim, w.porder)
     assert m.Init()
-    lz = sdt.BrwnLanczos(n3, w.max_iters, 1, w.lanczos_tol, reorth=True)
+    lz = sdt.BrwnLanczos(n3, max_iters or w.max_iters, 1, tol or w.lanczos_tol, reorth=True)
     assert lz.Init()
     st = sdt.StericForce(N, np.ones(N), w.box, w.steric_r0, w.steric_k0)
     assert st.Init()
@@ -133,6 +145,6 @@ def test_config3_first_ten_steps_vs_reference_trajectory(gpu_available):
         d = bd.get_positions() - pos0
         pk = P.astype(np.float64) @ d
         worst = max(worst, float(np.linalg.norm(pk - g["proj"][k]) / np.linalg.norm(g["proj"][k])))
-        assert abs(np.linalg.norm(d) / g["norms"][k] - 1.0) < 1e-4, k
-    assert worst < 1e-4, worst
+        assert abs(np.linalg.norm(d) / g["norms"][k] - 1.0) < bar, k
+    assert worst < bar, worst
     assert bd.info()["not_converged"] == 0

@@ -58,3 +58,82 @@ def test_noalloc_rejects_sizes_beyond_its_array(gpu_available):
                                         3 * N, ctypes.c_void_p(v.data_ptr()))
     assert st == -1
     assert b"262144" in L.sdt_spme_last_error(m.handle)
+
+
+def _noalloc(L, m, nr, alpha, ldf, f, beta, ldv, v):
+    st = L.sdt_spme_real_mulvec_noalloc(m.handle, nr, alpha, ldf, ctypes.c_void_p(f.data_ptr()), beta, ldv,
+                                        ctypes.c_void_p(v.data_ptr()))
+    assert st == 0, L.sdt_spme_last_error(m.handle)
+
+
+def test_noalloc_allocates_nothing_on_a_fresh_engine(gpu_available):
+    """On an engine that has never run a product (so it holds no product work
+    buffers), the first call leaves the device's free memory unchanged.  A
+    first call on another engine comes before, so the library's module is
+    loaded and the array's address looked up outside the measured call."""
+    import torch
+    import stokesdt_b200 as sdt
+    L = sdt.lib()
+    g = golden("spme_cfg1")
+    N = len(g["rdi"])
+    n3 = 3 * N
+    args = (N, g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
+    warm = sdt.MobSpme(*args)
+    assert warm.Init()
+    warm.Update(g["pos"])
+    f = torch.tensor(np.random.default_rng(3).standard_normal((2, n3)), device="cuda")
+    v = torch.zeros_like(f)
+    _noalloc(L, warm, 2, 1.0, n3, f, 0.0, n3, v)
+    warm.synchronize()
+    m = sdt.MobSpme(*args)
+    assert m.Init()
+    m.Update(g["pos"])
+    v_new = torch.zeros_like(f)
+    m.synchronize()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    _noalloc(L, m, 2, 1.0, n3, f, 0.0, n3, v_new)
+    m.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0, (free0, free1)
+    v_ref = torch.zeros_like(f)
+    m.mulvec_device(sdt.MODE_REAL, 2, 1.0, n3, f.data_ptr(), 0.0, n3, v_ref.data_ptr())
+    m.synchronize()
+    assert rel_err(v_ref.cpu().numpy(), v_new.cpu().numpy()) < TOL
+
+
+def test_noalloc_padded_leading_dimensions_and_in_place(gpu_available):
+    """ldf = ldv = 3N + 8 with beta != 0, against the allocating product on the
+    same padded buffers; then the same call in place (d_f == d_v)."""
+    import torch
+    import stokesdt_b200 as sdt
+    L = sdt.lib()
+    g = golden("spme_cfg1")
+    N = len(g["rdi"])
+    n3 = 3 * N
+    ld = n3 + 8
+    m = sdt.MobSpme(N, g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
+    assert m.Init()
+    m.Update(g["pos"])
+    rng = np.random.default_rng(29)
+    nr, alpha, beta = 3, 0.9, -0.4
+    f = torch.tensor(rng.standard_normal(nr * ld), device="cuda")
+    v0 = torch.tensor(rng.standard_normal(nr * ld), device="cuda")
+    v_ref, v_new = v0.clone(), v0.clone()
+    m.mulvec_device(sdt.MODE_REAL, nr, alpha, ld, f.data_ptr(), beta, ld, v_ref.data_ptr())
+    _noalloc(L, m, nr, alpha, ld, f, beta, ld, v_new)
+    m.synchronize()
+    ref = v_ref.cpu().numpy().reshape(nr, ld)
+    new = v_new.cpu().numpy().reshape(nr, ld)
+    assert rel_err(ref[:, :n3], new[:, :n3]) < TOL
+    # the padding between vectors is left alone
+    assert np.array_equal(new[:, n3:], v0.cpu().numpy().reshape(nr, ld)[:, n3:])
+    # in place: v := alpha M_real v + beta v
+    w_ref, w_new = f.clone(), f.clone()
+    tmp = f.clone()
+    m.mulvec_device(sdt.MODE_REAL, nr, alpha, ld, tmp.data_ptr(), beta, ld, w_ref.data_ptr())
+    _noalloc(L, m, nr, alpha, ld, w_new, beta, ld, w_new)
+    m.synchronize()
+    a = w_ref.cpu().numpy().reshape(nr, ld)[:, :n3]
+    b = w_new.cpu().numpy().reshape(nr, ld)[:, :n3]
+    assert rel_err(a, b) < TOL

@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--workload", default="cfg2",
                     help="cfg2 (default), cfg3 (trajectory), cfg4 (batch), cfg5 (served stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-interval", action="store_true",
+                    help="reference arm: skip the one whole measured interval (samples only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: a few mobility products, no timing output")
@@ -241,7 +243,87 @@ def cpu_sample(w, pos, its_hint):
 REF_ITERS = {"cfg2": 75}
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_full_interval(w, pos):
+    """One whole mobility interval through the reference's own code on all
+    host cores (BDSimBox::Advance, src/simbox/simbox_bd.cc:307-339):
+    MobSpme::Update, BrwnLanczos::Compute on 16 N(0,1) vectors (tol, 100
+    iterations at most), then 16 x { MulVector(1, dt, F_s, sqrt(2 dt), Y_s) ;
+    pos += Y_s }.  The reference's block Lanczos keeps ~21 MB on the stack
+    (src/brwn/brwn_lanczos.cc:97), so it runs on a thread with a 256 MB
+    stack.  Returns the wall time, the shim FFT's share and the iteration
+    count the reference logged."""
+    import threading
+    from oracle import ref
+    N, n3 = w.npos, 3 * w.npos
+    rdi = np.ones(N)
+    Z = np.random.default_rng(w.seed_z).standard_normal((INTERVAL, n3))
+    F = np.random.default_rng(w.seed_f).standard_normal((INTERVAL, n3))
+    out = {}
+
+    def run():
+        mob = ref.RefMob.spme(rdi, w.box, w.xi, w.rmax, w.dim, w.porder)
+        lz = ref.RefLanczos(n3, w.max_iters, INTERVAL, w.lanczos_tol)
+        p = np.ascontiguousarray(pos.reshape(-1), dtype=np.float64).copy()
+        ref.shim_fft_seconds(reset=True)
+        t0 = time.perf_counter()
+        mob.update(np.mod(p, w.box), rdi)
+        t1 = time.perf_counter()
+        Y, its = lz.compute(mob, Z)
+        t2 = time.perf_counter()
+        sq = math.sqrt(2.0 * DT)
+        for k in range(INTERVAL):
+            disp = mob.mulvec(F[k], DT, sq, Y[k])[0]
+            p += disp
+        t3 = time.perf_counter()
+        fft_s, calls = ref.shim_fft_seconds()
+        out.update(total_s=t3 - t0, update_s=t1 - t0, lanczos_s=t2 - t1, steps_s=t3 - t2, fft_s=fft_s,
+                   fft_calls=calls, iters=its)
+        mob.close()
+        lz.close()
+
+    threading.stack_size(256 << 20)
+    th = threading.Thread(target=run)
+    th.start()
+    th.join()
+    threading.stack_size(0)
+    return out
+
+
+def mkl_fft_pair_s(K: int) -> float:
+    """Seconds of one FP64 K^3 forward r2c plus backward c2r with torch's CPU
+    FFT (MKL-backed in this build) on all host threads: an MKL-class figure
+    for the transforms the reference runs through MKL DFTI."""
+    import torch
+    torch.set_num_threads(os.cpu_count() or 1)
+    x = torch.randn((K, K, K), dtype=torch.float64)
+    X = torch.fft.rfftn(x)
+    torch.fft.irfftn(X, s=(K, K, K))
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        X = torch.fft.rfftn(x)
+        torch.fft.irfftn(X, s=(K, K, K))
+    return (time.perf_counter() - t0) / reps
+
+
 def run_reference(args):
+    """The reference arm: the reference's own CPU path (oracle/_ref, built
+    from its unmodified sources) on this box's host cores.  Every timed step
+    is a bounded sample (Update + one 2-RHS MulVector) that gives the
+    extrapolated interval; after the timed steps one whole interval runs
+    through the reference's own Update, BrwnLanczos::Compute and MulVector,
+    and `value` is that measured interval (16 BD steps / its wall time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -250,21 +332,51 @@ def run_reference(args):
     pos = wl.rsa_positions(w.npos, w.box, w.seed_pos)
     its = REF_ITERS.get(args.workload) or 20
     samples = []
+    t_steps = 0.0
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         s = cpu_sample(w, pos, its)
         if i >= args.warmup:
             samples.append(s)
-    vals = [s["value"] for s in samples]
-    v = float(np.median(vals))
+            t_steps += time.perf_counter() - t0
+    v_extrap = float(np.median([s["value"] for s in samples]))
     base = dict(samples[-1])
-    base["value"] = v
+    cpu = {"value": v_extrap, "unit": UNIT, "cores": os.cpu_count(), "kind": base["kind"],
+           "sample": base["sample"], "cpu_model": cpu_model(),
+           "extrapolated_interval_s": round(INTERVAL / v_extrap, 3)}
+    value = v_extrap
+    if not args.no_full_interval and base["kind"] == "reference":
+        full = reference_full_interval(w, pos)
+        value = INTERVAL / full["total_s"]
+        mkl_pair = mkl_fft_pair_s(w.dim)
+        mkl_equiv = 0.5 * full["fft_calls"] * mkl_pair
+        adjusted = full["total_s"] - full["fft_s"] + mkl_equiv
+        cpu.update({
+            "value": value,
+            "measured_interval_s": round(full["total_s"], 3),
+            "measured_split_s": {"update": round(full["update_s"], 3), "lanczos": round(full["lanczos_s"], 3),
+                                 "16_steps": round(full["steps_s"], 3)},
+            "reference_lanczos_iters": full["iters"],
+            "measured_over_extrapolated": round(full["total_s"] / (INTERVAL / v_extrap), 4),
+            "fft_share": round(full["fft_s"] / full["total_s"], 4),
+            "fft_s": round(full["fft_s"], 3), "fft_calls": full["fft_calls"],
+            "mkl_class_fft_pair_s": round(mkl_pair, 4),
+            "fft_adjusted_interval_s": round(adjusted, 3),
+            "value_fft_adjusted": INTERVAL / adjusted,
+            "sample": (f"timed steps: {base['sample']}; value: one whole mobility interval measured through "
+                       f"the reference's own MobSpme::Update, BrwnLanczos::Compute (16 RHS, tol "
+                       f"{w.lanczos_tol}) and 16 MulVector calls on {os.cpu_count()} threads"),
+        })
+        log(f"reference interval: {full['total_s']:.1f} s measured vs {INTERVAL / v_extrap:.1f} s "
+            f"extrapolated; shim FFT {full['fft_s']:.1f} s of it")
     out = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * INTERVAL / v,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_steps / max(1, args.steps), 3),
+        "ms_per_interval": round(1e3 * INTERVAL / value, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(w),
-        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
-        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
 

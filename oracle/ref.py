@@ -66,6 +66,8 @@ def lib():
         L.sdtref_set_log.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.sdtref_set_log.restype = ctypes.c_int
         L.sdtref_close_log.argtypes = []
+        L.sdt_shim_fft_seconds.restype = ctypes.c_double
+        L.sdt_shim_fft_seconds.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
     return _lib
 
@@ -78,6 +80,14 @@ def _ptr(a: np.ndarray):
 def pad_len(n: int) -> int:
     """PadLen(n, sizeof(double)) of src/util/common.h:61-65 (multiple of 8)."""
     return (n + 7) // 8 * 8
+
+
+def shim_fft_seconds(reset: bool = False):
+    """(seconds, calls) spent in the DFTI stand-in's compute calls
+    (oracle/shim/dfti_fft.cc) since load or the last reset."""
+    calls = ctypes.c_longlong(0)
+    t = lib().sdt_shim_fft_seconds(1 if reset else 0, ctypes.byref(calls))
+    return float(t), int(calls.value)
 
 
 class RefMob:

@@ -370,18 +370,44 @@ static void Backward3D(SdtDftiDesc *d, double *data)
     }
 }
 
+// Wall time spent in the two compute calls since load (or the last reset),
+// so a timed reference run can report the share of its time this stand-in
+// FFT takes (it is not MKL).
+static double g_fft_seconds = 0.0;
+static long long g_fft_calls = 0;
+
+static double now_s() { return omp_get_wtime(); }
+
 MKL_LONG DftiComputeForward(DFTI_DESCRIPTOR_HANDLE d, void *inout, ...)
 {
     if (!d->committed) return 1;
+    const double t0 = now_s();
     Forward3D(d, (double *)inout);
+    g_fft_seconds += now_s() - t0;
+    g_fft_calls++;
     return 0;
 }
 
 MKL_LONG DftiComputeBackward(DFTI_DESCRIPTOR_HANDLE d, void *inout, ...)
 {
     if (!d->committed) return 1;
+    const double t0 = now_s();
     Backward3D(d, (double *)inout);
+    g_fft_seconds += now_s() - t0;
+    g_fft_calls++;
     return 0;
+}
+
+// Seconds and calls of the compute calls so far; reset != 0 zeroes them.
+double sdt_shim_fft_seconds(int reset, long long *calls)
+{
+    const double t = g_fft_seconds;
+    if (calls) *calls = g_fft_calls;
+    if (reset) {
+        g_fft_seconds = 0.0;
+        g_fft_calls = 0;
+    }
+    return t;
 }
 
 MKL_LONG DftiFreeDescriptor(DFTI_DESCRIPTOR_HANDLE *handle)

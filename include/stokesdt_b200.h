@@ -218,6 +218,20 @@ int sdt_batch_update(sdt_batch *h, const double *pos);
 int sdt_batch_mulvec(sdt_batch *h, int nrhs, double alpha, const double *f, double beta, double *v);
 int sdt_batch_lanczos(sdt_batch *h, int nrhs, const double *z, double *y, int *iters);
 
+/* Execution mode.  enable != 0 (the default when every system is
+ * monodisperse with grid dimension <= 256, reorthogonalisation is on and
+ * max_nrhs <= 16): every mobility product is one packed launch sequence over
+ * all systems (systems of one grid dimension share each grid-pass launch) and
+ * the block Lanczos iterates all systems in lockstep with batched Gram, GEMM
+ * and Cholesky-QR launches; each system leaves when its check passes.
+ * enable == 0: every system runs its own launches and the systems are spread
+ * over the lanes.  No counterpart in the reference, which runs
+ * src/mob/spme.cc:744-770 per system and per RHS.  SDT_ERR_UNSUPPORTED when
+ * the systems do not allow the packed mode. */
+int sdt_batch_set_packed(sdt_batch *h, int enable);
+/* 1 when the packed mode is selected, 0 otherwise. */
+int sdt_batch_get_packed(const sdt_batch *h);
+
 /* Total 3*sum(npos) and the lane count. */
 int sdt_batch_info(const sdt_batch *h, long long *total3n, int *lanes);
 int sdt_batch_synchronize(sdt_batch *h);

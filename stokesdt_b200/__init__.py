@@ -89,6 +89,8 @@ SIGNATURES = {
     "sdt_batch_lanczos": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _ip]),
     "sdt_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong), _ip]),
     "sdt_batch_synchronize": (ctypes.c_int, [_vp]),
+    "sdt_batch_set_packed": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "sdt_batch_get_packed": (ctypes.c_int, [_vp]),
     "sdt_batch_last_error": (ctypes.c_char_p, [_vp]),
     "sdt_batch_destroy": (None, [_vp]),
     "sdt_serve_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
@@ -578,6 +580,15 @@ class MobSpmeBatch:
 
     def synchronize(self):
         self._check(lib().sdt_batch_synchronize(self._h))
+
+    def set_packed(self, enable: bool):
+        """Packed launches over all systems (default where supported) or
+        every system's own launches spread over the lanes."""
+        self._check(lib().sdt_batch_set_packed(self._h, 1 if enable else 0))
+
+    @property
+    def packed(self) -> bool:
+        return lib().sdt_batch_get_packed(self._h) == 1
 
     def __del__(self):
         try:

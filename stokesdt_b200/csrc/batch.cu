@@ -13,8 +13,16 @@
 //
 // Vectors of all systems are concatenated: system s owns nrhs blocks of
 // 3*npos[s] doubles starting at offset nrhs * 3 * (npos[0] + ... + npos[s-1]).
+//
+// Packed mode (the default when every system is monodisperse with K <= 256
+// and reorthogonalisation is on): after the per-system updates, every
+// product is one packed launch sequence over all systems and the block
+// Lanczos runs all systems in lockstep (packed.h, packed_lanczos.h), so a
+// batch step takes tens of launches per Lanczos iteration instead of tens per
+// system and iteration.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -109,6 +117,66 @@ int batch_create(BatchState *b, int nsys, const int *npos, const double *rdi_all
         if (st != kOk) return batch_error(b, st, "Lanczos workspace: " + ln.lz->last_error);
         for (int s : ln.systems) b->sys[s].mob->stream = ln.stream;
     }
+    b->max_iters = max_iters;
+    b->max_nrhs = max_nrhs;
+    b->tol = tol;
+    b->packed_ok = b->reorth && max_nrhs <= kBlMaxK;
+    for (int s = 0; s < nsys && b->packed_ok; s++) {
+        const SpmeEngine *e = b->sys[s].mob;
+        if (!e->mono || e->K > 256 || !e->tma_tabs || !e->tma_enabled || !e->zfused) b->packed_ok = false;
+    }
+    const char *env = std::getenv("STOKESDT_BATCH_PACKED");
+    if (b->packed_ok && !(env && env[0] == '0')) return batch_set_packed(b, true);
+    return kOk;
+}
+
+int batch_set_packed(BatchState *b, bool packed)
+{
+    if (!packed) {
+        b->packed = false;
+        return kOk;
+    }
+    if (!b->packed_ok)
+        return batch_error(b, kErrUnsupported,
+                           "packed mode needs monodisperse systems with K <= 256, reorthogonalisation and "
+                           "at most 16 RHS per Lanczos group");
+    if (!b->pk) {
+        if (cudaSetDevice(b->device) != cudaSuccess) return batch_error(b, kErrCuda, "cudaSetDevice failed");
+        if (!b->pstream && cudaStreamCreateWithFlags(&b->pstream, cudaStreamNonBlocking) != cudaSuccess)
+            return batch_error(b, kErrCuda, "stream creation failed");
+        std::vector<SpmeEngine *> eng;
+        std::vector<int> npos;
+        for (SystemSlot &sl : b->sys) {
+            eng.push_back(sl.mob);
+            npos.push_back(sl.mob->npos);
+        }
+        b->pk = new PackedBatch;
+        int st = packed_create(b->pk, eng, std::max(1, b->max_nrhs), b->device, b->pstream);
+        if (st != kOk) {
+            const std::string msg = b->pk->last_error;
+            packed_free(b->pk);
+            delete b->pk;
+            b->pk = nullptr;
+            return batch_error(b, st, "packed set-up: " + msg);
+        }
+        b->bl = new BLState;
+        st = bl_create(b->bl, npos, b->max_iters, std::max(1, b->max_nrhs), b->tol, b->device, b->pstream);
+        if (st != kOk) {
+            const std::string msg = b->bl->last_error;
+            bl_free(b->bl);
+            delete b->bl;
+            b->bl = nullptr;
+            return batch_error(b, st, "batched Lanczos set-up: " + msg);
+        }
+    }
+    b->packed = true;
+    // the packed descriptors follow the engines' current positions
+    bool updated = true;
+    for (SystemSlot &sl : b->sys) updated = updated && sl.mob->updated;
+    if (updated) {
+        const int st = packed_refresh(b->pk);
+        if (st != kOk) return batch_error(b, st, b->pk->last_error);
+    }
     return kOk;
 }
 
@@ -145,13 +213,45 @@ static int for_each_system(BatchState *b, Fn &&fn)
 
 int batch_update(BatchState *b, const double *d_pos_all)
 {
-    return for_each_system(b, [&](int s, Lane &) {
+    if (b->packed) {
+        // the positions may come from work queued on the packed stream
+        if (cudaStreamSynchronize(b->pstream) != cudaSuccess)
+            return batch_error(b, kErrCuda, "packed stream synchronize failed");
+    }
+    int st = for_each_system(b, [&](int s, Lane &) {
         return spme_update(b->sys[s].mob, d_pos_all + b->pos_off[s]);
     });
+    if (st != kOk || !b->packed) return st;
+    for (Lane &ln : b->lanes)
+        if (ln.stream && cudaStreamSynchronize(ln.stream) != cudaSuccess)
+            return batch_error(b, kErrCuda, "stream synchronize failed");
+    st = packed_refresh(b->pk);
+    if (st != kOk) return batch_error(b, st, b->pk->last_error);
+    return kOk;
 }
 
 int batch_mulvec(BatchState *b, int nrhs, double alpha, const double *d_f_all, double beta, double *d_v_all)
 {
+    if (b->packed) {
+        std::vector<int> act(b->nsys);
+        std::vector<const double *> f(b->nsys);
+        std::vector<double *> v(b->nsys);
+        std::vector<int> ld(b->nsys);
+        for (int r0 = 0; r0 < nrhs; r0 += b->pk->rhs_cap) {
+            const int nr = std::min(b->pk->rhs_cap, nrhs - r0);
+            for (int s = 0; s < b->nsys; s++) {
+                const long long n3 = 3LL * b->sys[s].mob->npos;
+                act[s] = s;
+                f[s] = d_f_all + (long long)nrhs * b->pos_off[s] + r0 * n3;
+                v[s] = d_v_all + (long long)nrhs * b->pos_off[s] + r0 * n3;
+                ld[s] = (int)n3;
+            }
+            const int st = packed_mulvec(b->pk, b->nsys, act.data(), nr, alpha, f.data(), ld.data(), beta, v.data(),
+                                         ld.data());
+            if (st != kOk) return batch_error(b, st, b->pk->last_error);
+        }
+        return kOk;
+    }
     return for_each_system(b, [&](int s, Lane &) {
         SpmeEngine *e = b->sys[s].mob;
         const long long off = (long long)nrhs * b->pos_off[s];
@@ -162,6 +262,29 @@ int batch_mulvec(BatchState *b, int nrhs, double alpha, const double *d_f_all, d
 
 int batch_lanczos(BatchState *b, int nrhs, const double *d_z_all, double *d_y_all, int *iters)
 {
+    if (b->packed) {
+        std::vector<int> sel(b->nsys), ld(b->nsys), it(b->nsys, 0);
+        std::vector<const double *> z(b->nsys);
+        std::vector<double *> y(b->nsys);
+        int out = kOk;
+        // groups of max_nrhs RHS, as BrwnLanczos::Compute; iters[] reports the first
+        for (int r0 = 0; r0 < nrhs; r0 += b->max_nrhs) {
+            const int k = std::min(b->max_nrhs, nrhs - r0);
+            for (int s = 0; s < b->nsys; s++) {
+                const long long n3 = 3LL * b->sys[s].mob->npos;
+                sel[s] = s;
+                z[s] = d_z_all + (long long)nrhs * b->pos_off[s] + r0 * n3;
+                y[s] = d_y_all + (long long)nrhs * b->pos_off[s] + r0 * n3;
+                ld[s] = (int)n3;
+            }
+            const int st = bl_compute(b->bl, b->pk, sel, k, z.data(), ld.data(), y.data(), ld.data(), it.data());
+            if (st != kOk && st != kErrNotConverged) return batch_error(b, st, b->bl->last_error);
+            if (st == kErrNotConverged) out = kErrNotConverged;
+            if (r0 == 0 && iters)
+                for (int s = 0; s < b->nsys; s++) iters[s] = it[s];
+        }
+        return out;
+    }
     return for_each_system(b, [&](int s, Lane &ln) {
         SpmeEngine *e = b->sys[s].mob;
         const long long off = (long long)nrhs * b->pos_off[s];
@@ -179,6 +302,10 @@ int batch_lanczos(BatchState *b, int nrhs, const double *d_z_all, double *d_y_al
 int batch_synchronize(BatchState *b)
 {
     if (cudaSetDevice(b->device) != cudaSuccess) return batch_error(b, kErrCuda, "cudaSetDevice failed");
+    if (b->pk) {
+        const int st = packed_check_error(b->pk);
+        if (st != kOk) return batch_error(b, st, b->pk->last_error);
+    }
     for (Lane &ln : b->lanes)
         if (ln.stream && cudaStreamSynchronize(ln.stream) != cudaSuccess)
             return batch_error(b, kErrCuda, "stream synchronize failed");
@@ -193,6 +320,18 @@ void batch_free(BatchState *b)
 {
     if (!b) return;
     cudaSetDevice(b->device);
+    if (b->bl) {
+        bl_free(b->bl);
+        delete b->bl;
+        b->bl = nullptr;
+    }
+    if (b->pk) {
+        packed_free(b->pk);
+        delete b->pk;
+        b->pk = nullptr;
+    }
+    if (b->pstream) cudaStreamDestroy(b->pstream);
+    b->pstream = nullptr;
     for (Lane &ln : b->lanes)
         if (ln.stream) cudaStreamSynchronize(ln.stream);
     for (SystemSlot &sl : b->sys) {

@@ -8,6 +8,8 @@
 
 #include "engine.h"
 #include "lanczos.h"
+#include "packed.h"
+#include "packed_lanczos.h"
 
 namespace sdt {
 
@@ -31,8 +33,21 @@ struct BatchState {
     std::vector<long long> pos_off;  // [nsys + 1] offsets of 3N blocks
     double *d_stage = nullptr;       // host-API staging (grown on demand)
     size_t stage_cap = 0;
+    // packed mode (default when every system qualifies): products and block
+    // Lanczos of all systems as packed launches on one stream (packed.h);
+    // lanes mode: every system's own launches, systems spread over the lanes
+    bool packed_ok = false;          // the systems allow the packed mode
+    bool packed = false;             // packed mode selected
+    int max_iters = 0, max_nrhs = 0;
+    double tol = 0.0;
+    cudaStream_t pstream = nullptr;
+    PackedBatch *pk = nullptr;
+    BLState *bl = nullptr;
     std::string last_error;
 };
+
+// 1: packed launches (needs monodisperse systems with K <= 256), 0: lanes.
+int batch_set_packed(BatchState *b, bool packed);
 
 int batch_create(BatchState *b, int nsys, const int *npos, const double *rdi_all, const double *box,
                  const int *dim, const double *xi, const double *rmax, int porder, int max_iters,

@@ -162,6 +162,18 @@ int sdt_batch_info(const sdt_batch *h, long long *total3n, int *lanes)
     return SDT_OK;
 }
 
+int sdt_batch_set_packed(sdt_batch *h, int enable)
+{
+    if (!h) return SDT_ERR_INVALID;
+    return sdt::batch_set_packed(&h->b, enable != 0);
+}
+
+int sdt_batch_get_packed(const sdt_batch *h)
+{
+    if (!h) return SDT_ERR_INVALID;
+    return h->b.packed ? 1 : 0;
+}
+
 int sdt_batch_synchronize(sdt_batch *h)
 {
     if (!h) return SDT_ERR_INVALID;

@@ -187,6 +187,8 @@ int spme_spectrum(SpmeEngine *e, int nrhs, int ldf, const double *d_f, float *d_
 int real_space_launch(SpmeEngine *e, int rb);
 // Same with caller-supplied buffers: fs [N][nr][3] (cell order), vreal [nr][3N].
 int real_space_launch_into(SpmeEngine *e, int nr, const float *fs, float *vreal);
+// Cell walk with float4 force rows fs [N][nr] (cell order) on stream s.
+int real_space_walk_into4(SpmeEngine *e, int nr, const float4 *fs, float *vreal, cudaStream_t s);
 // Build / release the real-space pair list (used by real_space_launch when
 // pl_ready).
 int pair_list_build(SpmeEngine *e);

@@ -33,6 +33,7 @@
 // read that source's RB force vectors as one contiguous float4 row.  Partial
 // sums of one right-hand side are reduced over the sub-slots with shuffles.
 #include "engine.h"
+#include "packed.h"
 
 namespace sdt {
 
@@ -354,11 +355,12 @@ __global__ void __launch_bounds__(1024) k_scan64(int n, const int *__restrict__ 
 // one batch ahead of the one it applies, and stages the current batch in
 // shared memory; a batch takes RB steps of 32/RB pairs, whose force loads are
 // issued kFB at a time before the math.
+// The work of one CTA: targets block * kRsWarps + warp.
 template <int RB>
-__global__ void __launch_bounds__(32 * kRsWarps, 2)
-k_pair_apply(int n, const long long *__restrict__ start, const float4 *__restrict__ pl_e,
-             const float2 *__restrict__ pl_c, const int *__restrict__ perm,
-             const float4 *__restrict__ fs, int nr, int r0, float *__restrict__ vreal)
+__device__ __forceinline__ void pair_apply_block(int n, const long long *__restrict__ start,
+                                                 const float4 *__restrict__ pl_e, const float2 *__restrict__ pl_c,
+                                                 const int *__restrict__ perm, const float4 *__restrict__ fs,
+                                                 int nr, int r0, float *__restrict__ vreal, int block)
 {
     static_assert(RB >= 1 && RB <= 32 && (32 % RB) == 0, "RB must divide the warp");
     constexpr int kPairsPerStep = 32 / RB;
@@ -366,7 +368,7 @@ k_pair_apply(int n, const long long *__restrict__ start, const float4 *__restric
     __shared__ float4 se[kRsWarps][32];
     __shared__ float2 sc[kRsWarps][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = blockIdx.x * kRsWarps + warp;
+    const int s = block * kRsWarps + warp;
     if (s >= n) return;
     const int rl = lane % RB, pl = lane / RB;
     const float4 *frow = fs + r0 + rl;
@@ -411,6 +413,28 @@ k_pair_apply(int n, const long long *__restrict__ start, const float4 *__restric
         }
     }
     store_rows<RB>(a0, a1, a2, lane, perm[s], n, r0, vreal);
+}
+
+template <int RB>
+__global__ void __launch_bounds__(32 * kRsWarps, 2)
+k_pair_apply(int n, const long long *__restrict__ start, const float4 *__restrict__ pl_e,
+             const float2 *__restrict__ pl_c, const int *__restrict__ perm,
+             const float4 *__restrict__ fs, int nr, int r0, float *__restrict__ vreal)
+{
+    pair_apply_block<RB>(n, start, pl_e, pl_c, perm, fs, nr, r0, vreal, blockIdx.x);
+}
+
+// Packed over many systems: CTA blockIdx.x takes block map[blockIdx.x].y of
+// the system in slot map[blockIdx.x].x.
+template <int RB>
+__global__ void __launch_bounds__(32 * kRsWarps, 2)
+k_pair_apply_packed(const PackedSys *__restrict__ sys, const PackedIO *__restrict__ io,
+                    const int *__restrict__ act, const int2 *__restrict__ map, int nr, int r0)
+{
+    const int2 m = map[blockIdx.x];
+    const int g = act[m.x];
+    const PackedSys &S = sys[g];
+    pair_apply_block<RB>(S.n, S.pl_start, S.pl_e, S.pl_c, S.rs_perm, io[g].fs_rs, nr, r0, io[g].vreal, m.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -508,6 +532,44 @@ int real_space_launch_into(SpmeEngine *e, int nr, const float *fs, float *vreal)
 {
     const int grid = (e->npos + kRsWarps - 1) / kRsWarps;
     return for_rhs_blocks(nr, WalkLaunch<3>{e, cell_walk(e), grid, nr, fs, vreal});
+}
+
+// The same with float4 force rows ([N][nr] float4, cell order) on stream s:
+// the packed path's fallback for a system without a stored pair list.
+int real_space_walk_into4(SpmeEngine *e, int nr, const float4 *fs, float *vreal, cudaStream_t s)
+{
+    const int grid = (e->npos + kRsWarps - 1) / kRsWarps;
+    cudaStream_t saved = e->stream;
+    e->stream = s;
+    const int st =
+        for_rhs_blocks(nr, WalkLaunch<4>{e, cell_walk(e), grid, nr, reinterpret_cast<const float *>(fs), vreal});
+    e->stream = saved;
+    return st;
+}
+
+int packed_pair_targets_per_cta() { return kRsWarps; }
+
+struct PackedPairLaunch {
+    const PackedSys *sys;
+    const PackedIO *io;
+    const int *act;
+    const int2 *map;
+    int nblocks, nr;
+    cudaStream_t s;
+    template <int RB>
+    int run(int r0) const
+    {
+        k_pair_apply_packed<RB><<<nblocks, 32 * kRsWarps, 0, s>>>(sys, io, act, map, nr, r0);
+        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+        return cudaGetLastError() == cudaSuccess ? kOk : kErrCuda;
+    }
+};
+
+int packed_pair_apply(const PackedSys *d_sys, const PackedIO *d_io, const int *d_act, const int2 *d_map,
+                      int nblocks, int nr, cudaStream_t s)
+{
+    if (nblocks <= 0) return kOk;
+    return for_rhs_blocks(nr, PackedPairLaunch{d_sys, d_io, d_act, d_map, nblocks, nr, s});
 }
 
 // Build the pair list for the current positions (after the cell sort of

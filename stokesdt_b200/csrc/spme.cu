@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "packed.h"
 #include "fft.cuh"
 #include "tma.cuh"
 #include "rowblock.cuh"
@@ -364,21 +365,20 @@ __device__ __forceinline__ float2 c2r_merge(float2 xk, float2 xm, float2 w)
 // block into kXRows shared-memory rows (component-major), FFT every row along x
 // (real-to-complex) and write the half spectra.  Each row segment's index
 // data and weights are loaded once for its 3 x p atomics.
+// The work of one CTA: RHS r, row block (by, bz).
 template <int K>
-__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
-k_spread_xfwd(int n, int p, int nby, const int *__restrict__ seg_start,
-              const unsigned *__restrict__ seg_meta, const int *__restrict__ seg_slot,
-              const float *__restrict__ seg_w, const float *__restrict__ sp_w,
-              const float *__restrict__ fs_sp, int XS, const float2 *__restrict__ tw_half,
-              const float2 *__restrict__ tw_full, float2 *__restrict__ cgrid, int r0)
+__device__ __forceinline__ void spread_xfwd_block(int n, int p, int nby, const int *__restrict__ seg_start,
+                                                  const unsigned *__restrict__ seg_meta,
+                                                  const int *__restrict__ seg_slot, const float *__restrict__ seg_w,
+                                                  const float *__restrict__ sp_w, const float *__restrict__ fs_sp,
+                                                  int XS, const float2 *__restrict__ tw_half,
+                                                  const float2 *__restrict__ tw_full, float2 *__restrict__ cgrid,
+                                                  int r, int by, int bz)
 {
     constexpr int H = K / 2;
     constexpr int NRB = kRowBlockY * kRowBlockZ;
     static_assert(x_rows_fit<K>(), "rows fit the footprint");
     extern __shared__ __align__(128) float rows[];  // kXRows rows at x_row_offset<K>
-    // the RHS index runs fastest, so the CTAs of one row block run together
-    // and share its segment lists and weights through L2
-    const int r = r0 + blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
     const int tid = threadIdx.x;
     {
         float4 *r4 = reinterpret_cast<float4 *>(rows);
@@ -513,6 +513,35 @@ k_spread_xfwd(int n, int p, int nby, const int *__restrict__ seg_start,
             }
         }
     }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
+k_spread_xfwd(int n, int p, int nby, const int *__restrict__ seg_start,
+              const unsigned *__restrict__ seg_meta, const int *__restrict__ seg_slot,
+              const float *__restrict__ seg_w, const float *__restrict__ sp_w,
+              const float *__restrict__ fs_sp, int XS, const float2 *__restrict__ tw_half,
+              const float2 *__restrict__ tw_full, float2 *__restrict__ cgrid, int r0)
+{
+    // the RHS index runs fastest, so the CTAs of one row block run together
+    // and share its segment lists and weights through L2
+    spread_xfwd_block<K>(n, p, nby, seg_start, seg_meta, seg_slot, seg_w, sp_w, fs_sp, XS, tw_half, tw_full, cgrid,
+                         r0 + blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Packed: blockIdx.z = slot * nbz + bz; the slot's system and grid slice
+// come from the class's slot table.
+template <int K>
+__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
+k_spread_xfwd_packed(const PackedSys *__restrict__ sys, const PackedIO *__restrict__ io,
+                     const int *__restrict__ slot_sys, int nbz, int XS, const float2 *__restrict__ tw_half,
+                     const float2 *__restrict__ tw_full, float2 *__restrict__ grid, long long slot_stride)
+{
+    const int slot = blockIdx.z / nbz, bz = blockIdx.z - slot * nbz;
+    const int g = slot_sys[slot];
+    const PackedSys &S = sys[g];
+    spread_xfwd_block<K>(S.n, S.p, S.nby, S.seg_start, S.seg_meta, S.seg_slot, S.seg_w, S.sp_w, io[g].fs_sp, XS,
+                         tw_half, tw_full, grid + (size_t)slot * slot_stride, blockIdx.x, blockIdx.y, bz);
 }
 
 // Complex FFT along y of a 16-column kx tile of one z-plane, in place.
@@ -730,23 +759,23 @@ k_zpass_influence_tma(const __grid_constant__ CUtensorMap map, const __grid_cons
 // pairs (k, H-k) of its step-1 samples in registers and the transform
 // writes the row at x_row_offset.  Otherwise each warp loads its rows and
 // merges them on the way into shared memory before the transform.
+// The work of one CTA: RHS r, row block (by, bz).
 template <int K, bool BULK>
-__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
-k_xinv_interp(int n, int p, int nby, const int *__restrict__ seg_start,
-              const unsigned *__restrict__ seg_meta, const int *__restrict__ seg_slot,
-              const float *__restrict__ seg_w, const float *__restrict__ sp_w,
-              const int *__restrict__ sp_perm, const double *__restrict__ iscale, int XS,
-              const float2 *__restrict__ tw_half, const float2 *__restrict__ tw_full,
-              const float2 *__restrict__ cgrid, float *__restrict__ vrecip, int r0, int *err)
+__device__ __forceinline__ void xinv_interp_block(int n, int p, int nby, const int *__restrict__ seg_start,
+                                                  const unsigned *__restrict__ seg_meta,
+                                                  const int *__restrict__ seg_slot, const float *__restrict__ seg_w,
+                                                  const float *__restrict__ sp_w, const int *__restrict__ sp_perm,
+                                                  const double *__restrict__ iscale, int XS,
+                                                  const float2 *__restrict__ tw_half,
+                                                  const float2 *__restrict__ tw_full,
+                                                  const float2 *__restrict__ cgrid, float *__restrict__ vrecip,
+                                                  int *err, int r, int by, int bz)
 {
     constexpr int H = K / 2;
     constexpr int NRB = kRowBlockY * kRowBlockZ;
     constexpr uint32_t kStageBytes = (uint32_t)((H + 2) * sizeof(float2));
     static_assert(kStageBytes % 16 == 0 && x_rows_fit<K>(), "staged rows fit the footprint");
     extern __shared__ __align__(128) float rows[];  // kXRows rows at x_row_offset<K>
-    // the RHS index runs fastest, so the CTAs of one row block run together
-    // and share its segment lists and weights through L2
-    const int r = r0 + blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     auto spectrum_row = [&](int rr) {
@@ -950,6 +979,37 @@ k_xinv_interp(int n, int p, int nby, const int *__restrict__ seg_start,
     }
 }
 
+template <int K, bool BULK>
+__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
+k_xinv_interp(int n, int p, int nby, const int *__restrict__ seg_start,
+              const unsigned *__restrict__ seg_meta, const int *__restrict__ seg_slot,
+              const float *__restrict__ seg_w, const float *__restrict__ sp_w,
+              const int *__restrict__ sp_perm, const double *__restrict__ iscale, int XS,
+              const float2 *__restrict__ tw_half, const float2 *__restrict__ tw_full,
+              const float2 *__restrict__ cgrid, float *__restrict__ vrecip, int r0, int *err)
+{
+    // the RHS index runs fastest, so the CTAs of one row block run together
+    // and share its segment lists and weights through L2
+    xinv_interp_block<K, BULK>(n, p, nby, seg_start, seg_meta, seg_slot, seg_w, sp_w, sp_perm, iscale, XS, tw_half,
+                               tw_full, cgrid, vrecip, err, r0 + blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Packed: blockIdx.z = slot * nbz + bz (see k_spread_xfwd_packed).
+template <int K>
+__global__ void __launch_bounds__(kXThreads, kXpassMinBlocks<K>())
+k_xinv_interp_packed(const PackedSys *__restrict__ sys, const PackedIO *__restrict__ io,
+                     const int *__restrict__ slot_sys, int nbz, int XS, const float2 *__restrict__ tw_half,
+                     const float2 *__restrict__ tw_full, const float2 *__restrict__ grid, long long slot_stride,
+                     int *err)
+{
+    const int slot = blockIdx.z / nbz, bz = blockIdx.z - slot * nbz;
+    const int g = slot_sys[slot];
+    const PackedSys &S = sys[g];
+    xinv_interp_block<K, true>(S.n, S.p, S.nby, S.seg_start, S.seg_meta, S.seg_slot, S.seg_w, S.sp_w, S.sp_perm,
+                               nullptr, XS, tw_half, tw_full, grid + (size_t)slot * slot_stride, io[g].vrecip, err,
+                               blockIdx.x, blockIdx.y, bz);
+}
+
 // v := alpha * (recip/L^3 + real + self*f) + beta * v, FP64.
 __global__ void k_combine(int n3, int nr, int mode, double alpha, double beta, double invL3,
                           const double *__restrict__ f, int ldf, const double *__restrict__ self,
@@ -980,10 +1040,14 @@ __host__ __device__ constexpr int kZFusedThreads() { return kTileZF * FftShape<K
 // FWD_ONLY stops after the forward z transform and stores the spectrum (the
 // forward-transform diagnostic sdt_spme_spectrum_device); the product uses
 // FWD_ONLY = false.
-template <int K, bool FWD_ONLY = false>
+// PACKED: blockIdx.x = slot * nr + r runs over the slots of a packed class
+// grid; the slot's influence table (4D map, outermost coordinate = table
+// index) and wave numbers come from slot_tab.
+template <int K, bool FWD_ONLY = false, bool PACKED = false>
 __global__ void __launch_bounds__(kZFusedThreads<K>(), 6)
 k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap tabmap,
-                  const float2 *__restrict__ tw, const float *__restrict__ kmap, int *err, int r0)
+                  const float2 *__restrict__ tw, const float *__restrict__ kmap, int *err, int r0,
+                  const int *__restrict__ slot_tab = nullptr, int nr_packed = 1)
 {
     constexpr int H = K / 2;
     constexpr int N1 = FftShape<K>::N1, N2 = FftShape<K>::N2, NR = N1 / N2;
@@ -996,6 +1060,11 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
     const int r = r0 + blockIdx.x, tx = blockIdx.y, y = blockIdx.z;
     const int tid = threadIdx.x;
     const int kx0 = tx * kTileZF;
+    int tabi = 0;
+    if constexpr (PACKED) {
+        tabi = slot_tab[blockIdx.x / nr_packed];
+        kmap += (size_t)tabi * K;
+    }
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_barrier_init();
@@ -1006,8 +1075,12 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
         for (int c = 0; c < 3; c++)
             for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
                 tma_load_4d(sm + c * CS + z0 * kTileZF, &map, &bar, kx0, y, z0, 3 * r + c);
-        for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
-            tma_load_3d(tabs + z0 * kTileZF, &tabmap, &bar, kx0, y, z0);
+        for (int z0 = 0; z0 < K; z0 += kTmaBoxLines) {
+            if constexpr (PACKED)
+                tma_load_4d(tabs + z0 * kTileZF, &tabmap, &bar, kx0, y, z0, tabi);
+            else
+                tma_load_3d(tabs + z0 * kTileZF, &tabmap, &bar, kx0, y, z0);
+        }
     }
     const bool ok = mbar_wait(&bar, 0);
     if (!__syncthreads_and(ok)) {
@@ -1741,6 +1814,110 @@ void spme_free(SpmeEngine *e)
     e->ev_fork = nullptr;
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     e->stream = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Packed multi-system passes (packed.h): one launch per pass and grid class
+// ---------------------------------------------------------------------------
+
+#define PK_LAUNCH_CHECK()                                                                 \
+    do {                                                                                  \
+        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);                        \
+        if (cudaGetLastError() != cudaSuccess) return kErrCuda;                           \
+    } while (0)
+
+static long long packed_slot_stride(const PackedClass &c, int nr)
+{
+    return (long long)nr * 3 * c.K * c.K * c.XS;
+}
+
+template <int K>
+static int packed_x_spread_k(const PackedClass &c, const PackedSys *d_sys, const PackedIO *d_io, int nslots,
+                             int nr, cudaStream_t s)
+{
+    const size_t smx = (size_t)x_rows_floats<K>() * sizeof(float);
+    if (cudaFuncSetAttribute(k_spread_xfwd_packed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) !=
+        cudaSuccess)
+        return kErrCuda;
+    k_spread_xfwd_packed<K><<<dim3(nr, c.nby, c.nbz * nslots), kXThreads, smx, s>>>(
+        d_sys, d_io, c.d_slot_sys, c.nbz, c.XS, c.tw_half, c.tw_full, c.d_grid, packed_slot_stride(c, nr));
+    PK_LAUNCH_CHECK();
+    return kOk;
+}
+
+template <int K>
+static int packed_x_interp_k(const PackedClass &c, const PackedSys *d_sys, const PackedIO *d_io, int nslots,
+                             int nr, int *err, cudaStream_t s)
+{
+    const size_t smx = (size_t)x_rows_floats<K>() * sizeof(float);
+    if (cudaFuncSetAttribute(k_xinv_interp_packed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) !=
+        cudaSuccess)
+        return kErrCuda;
+    k_xinv_interp_packed<K><<<dim3(nr, c.nby, c.nbz * nslots), kXThreads, smx, s>>>(
+        d_sys, d_io, c.d_slot_sys, c.nbz, c.XS, c.tw_half, c.tw_full, c.d_grid, packed_slot_stride(c, nr), err);
+    PK_LAUNCH_CHECK();
+    return kOk;
+}
+
+template <int K>
+static int packed_y_k(const PackedClass &c, int nslots, int nr, bool inverse, int *err, cudaStream_t s)
+{
+    constexpr int H = K / 2;
+    const size_t smy = (size_t)K * kTileX * sizeof(float2);
+    const int ntile = (H + 1 + kTileX - 1) / kTileX;
+    const int ty = kTileX * FftShape<K>::N2;
+    auto kern = inverse ? k_ypass_tma<K, true> : k_ypass_tma<K, false>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) != cudaSuccess)
+        return kErrCuda;
+    kern<<<dim3(ntile, K, nr * 3 * nslots), ty, smy, s>>>(c.tmap_y, c.tw_full, err, 0);
+    PK_LAUNCH_CHECK();
+    return kOk;
+}
+
+template <int K>
+static int packed_z_k(const PackedClass &c, int nslots, int nr, int *err, cudaStream_t s)
+{
+    constexpr int H = K / 2;
+    const size_t smzf = (size_t)3 * K * kTileZF * sizeof(float2) + (size_t)K * kTileZF * sizeof(float);
+    const int ntilezf = (H + 1 + kTileZF - 1) / kTileZF;
+    auto kern = k_zpass_fused_tma<K, false, true>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smzf) != cudaSuccess)
+        return kErrCuda;
+    kern<<<dim3(nr * nslots, ntilezf, K), kZFusedThreads<K>(), smzf, s>>>(c.tmap_zf, c.tmap_tabf, c.tw_full,
+                                                                         c.d_kmap, err, 0, c.d_slot_tab, nr);
+    PK_LAUNCH_CHECK();
+    return kOk;
+}
+
+#define PK_DISPATCH(fn, ...)                                                              \
+    switch (c.K) {                                                                        \
+        case 32: return fn<32>(__VA_ARGS__);                                              \
+        case 64: return fn<64>(__VA_ARGS__);                                              \
+        case 128: return fn<128>(__VA_ARGS__);                                            \
+        case 256: return fn<256>(__VA_ARGS__);                                            \
+        default: return kErrUnsupported;                                                  \
+    }
+
+int packed_x_spread(const PackedClass &c, const PackedSys *d_sys, const PackedIO *d_io, int nslots, int nr,
+                    cudaStream_t s)
+{
+    PK_DISPATCH(packed_x_spread_k, c, d_sys, d_io, nslots, nr, s)
+}
+
+int packed_x_interp(const PackedClass &c, const PackedSys *d_sys, const PackedIO *d_io, int nslots, int nr,
+                    int *err, cudaStream_t s)
+{
+    PK_DISPATCH(packed_x_interp_k, c, d_sys, d_io, nslots, nr, err, s)
+}
+
+int packed_y(const PackedClass &c, int nslots, int nr, bool inverse, int *err, cudaStream_t s)
+{
+    PK_DISPATCH(packed_y_k, c, nslots, nr, inverse, err, s)
+}
+
+int packed_z(const PackedClass &c, int nslots, int nr, int *err, cudaStream_t s)
+{
+    PK_DISPATCH(packed_z_k, c, nslots, nr, err, s)
 }
 
 }  // namespace sdt

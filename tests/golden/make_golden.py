@@ -26,6 +26,8 @@ Cases (reference test that each one follows):
                       (tol 1e-6, max_iters 100, 16 RHS) on the reference's MobSpme;
                       the iteration count and 64 random projections of the first two
                       Brownian vectors (--cfg2 only: ~15 minutes on 8 cores)
+  batch_sys6          6 autotuned batch systems (N in [300, 3000]): MobSpme MulVector on 3 RHS
+                      (alpha 0.8, beta 0.5) per system (--batch only)
   mf_cfg2_proj        config 2 at full size: MobSpme MulVector / RealMulVector /
                       RecipMulVector on 4 RHS (alpha 1.3, beta 0.7); 64 random projections,
                       norms and the first 512 particles' outputs per mode (--mf-cfg2 only)
@@ -250,11 +252,36 @@ def mf_cfg2_case(name):
                         head=np.array(MF_CFG2_HEAD), **out)
 
 
+def batch_sys_case(name):
+    """Config-4-style batch (6 systems, N log-uniform in [300, 3000], grid and
+    Ewald split by the autotuner, seed 8): the reference's MobSpme MulVector
+    (alpha 0.8, beta 0.5, 3 RHS) for each system, so a packed batch product is
+    checked against the reference on every system."""
+    from stokesdt_b200 import workloads as wl
+    sy = wl.batch_systems(nsys=6, seed=8, nmin=300, nmax=3000)
+    out = {}
+    for s, d in enumerate(sy):
+        N, n3 = d["npos"], 3 * d["npos"]
+        pos = wl.rsa_positions(N, d["box"], d["seed"])
+        rng = np.random.default_rng(500 + s)
+        f = rng.standard_normal((3, n3))
+        v0 = rng.standard_normal((3, n3))
+        sp = ref.RefMob.spme(np.ones(N), d["box"], d["xi"], d["rmax"], d["K"], 6)
+        sp.update(pos, np.ones(N))
+        out[f"f{s}"] = f
+        out[f"v0_{s}"] = v0
+        out[f"v{s}"] = sp.mulvec(f, 0.8, 0.5, v0.copy())
+        print(f"{name}: system {s} N={N} K={d['K']}")
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), nsys=np.array(len(sy)), alpha=np.array(0.8),
+                        beta=np.array(0.5), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--cfg2", action="store_true", help="only the config-2 Lanczos fixture")
     ap.add_argument("--mf-cfg2", action="store_true", help="only the config-2 mobility-product fixture")
+    ap.add_argument("--batch", action="store_true", help="only the batch-systems fixture")
     ap.add_argument("--lanczos", action="store_true", help="only the N1000 Lanczos fixture")
     ap.add_argument("--steric", action="store_true", help="only the steric-force fixtures")
     ap.add_argument("--bd", action="store_true", help="only the config-3 trajectory fixture")
@@ -275,6 +302,9 @@ def main():
         return
     if a.mf_cfg2:
         mf_cfg2_case("mf_cfg2_proj")
+        return
+    if a.batch:
+        batch_sys_case("batch_sys6")
         return
     if a.lanczos:
         pos, rdi, L = ref.parse_xyz(os.path.join(a.ref, "tests", "data", "N1000_Phi0.1.xyz"))

@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--no-full-interval", action="store_true",
                     help="reference arm: skip the one whole measured interval (samples only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="config 4: skip the lanes-mode and plain per-system comparison legs")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: a few mobility products, no timing output")
     ap.add_argument("--profile-rhs", type=int, default=1, help="RHS per product in --profile-case")
@@ -796,6 +798,14 @@ def run_b200_batch(args):
         b.synchronize()
         return its
 
+    if args.profile_case:
+        # small case for ncu launch lists: an update and two 4-RHS packed products
+        b.update_device(d_pos.data_ptr())
+        for _ in range(2):
+            b.mulvec_device(4, 1.0, d_Z.data_ptr(), 0.0, d_Y.data_ptr())
+        b.synchronize()
+        return
+
     def barrier():
         torch.cuda.synchronize(dev)
         if dist is not None:
@@ -822,6 +832,24 @@ def run_b200_batch(args):
     total_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[-1]), dev)
     value = total * args.steps / (total_ms / 1e3)
 
+    packed = b.packed
+    # per-phase wall time of one more step (synchronised between phases)
+    phase = {}
+    barrier()
+    t0 = time.perf_counter()
+    b.update_device(d_pos.data_ptr())
+    b.synchronize()
+    t1 = time.perf_counter()
+    b.mulvec_device(1, 1.0, d_F.data_ptr(), 0.0, d_V.data_ptr())
+    b.synchronize()
+    t2 = time.perf_counter()
+    b.lanczos_device(4, d_Z.data_ptr(), d_Y.data_ptr())
+    b.synchronize()
+    t3 = time.perf_counter()
+    phase = {"update": round(1e3 * (t1 - t0), 1), "mf_1rhs": round(1e3 * (t2 - t1), 1),
+             "lanczos_4rhs": round(1e3 * (t3 - t2), 1)}
+    log(f"config 4 phases (ms): {phase}")
+
     e2e = None
     if not args.no_e2e:
         hF = torch.tensor(d_F.cpu().numpy()).pin_memory().numpy()
@@ -843,6 +871,51 @@ def run_b200_batch(args):
         e2e = {"value": total * ke / (e_ms / 1e3), "unit": "systems/s",
                "h2d_bytes_per_step": 8 * (len(pos) + tot + 4 * tot),
                "d2h_bytes_per_step": 8 * (tot + 4 * tot), "steps": ke}
+
+    # the same step with every system's own launches spread over the lanes,
+    # then the plain per-system path: each system through the single-system
+    # API (MobSpme + BrwnLanczos), one after the other
+    def timed(fn, reps):
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return (time.perf_counter() - t0) / reps
+
+    lanes_rate = None
+    if packed and not args.no_compare:
+        b.set_packed(False)
+        step()
+        lanes_rate = len(mine) / timed(step, max(1, min(args.steps, 2)))
+        b.set_packed(True)
+    del b
+    torch.cuda.empty_cache()
+    plain_rate = None
+    if not args.no_compare:
+        engines = []
+        for i, s in enumerate(sy):
+            m = sdt.MobSpme(s["npos"], np.ones(s["npos"]), s["box"], s["xi"], s["rmax"], s["K"], 6, device=local)
+            assert m.Init()
+            m.set_stream(stream.cuda_stream)
+            lz = sdt.BrwnLanczos(3 * s["npos"], 100, 4, 1e-6, device=local, reorth=True)
+            assert lz.Init()
+            lz.set_stream(stream.cuda_stream)
+            engines.append((m, lz))
+        off = np.concatenate([[0], np.cumsum([3 * s["npos"] for s in sy])])
+
+        def plain_step():
+            for i, (m, lz) in enumerate(engines):
+                n3 = int(off[i + 1] - off[i])
+                m.update_device(d_pos.data_ptr() + 8 * int(off[i]))
+                m.mulvec_device(0, 1, 1.0, n3, d_F.data_ptr() + 8 * int(off[i]), 0.0, n3,
+                                d_V.data_ptr() + 8 * int(off[i]))
+                lz.compute_device(m, 4, n3, d_Z.data_ptr() + 32 * int(off[i]), n3,
+                                  d_Y.data_ptr() + 32 * int(off[i]))
+
+        plain_step()
+        plain_rate = len(mine) / timed(plain_step, 1)
+        del engines
     if rank == 0:
         lat = np.array(step_ms)
         out = {
@@ -853,8 +926,14 @@ def run_b200_batch(args):
             "config": {"workload": "256 systems, N log-uniform [500, 20000], phi U[0.05, 0.3], K per system "
                                    "(autotuned, 64/128), p=6, 1 M.f + 4-RHS Lanczos tol 1e-6 each",
                        "systems": total, "particles": int(sum(s["npos"] for s in systems)),
+                       "mode": "packed launches over all systems" if packed else "lanes",
                        "lanes_per_gpu": 8, "parallelism": f"systems sharded over {world} GPU(s)",
                        "l2": "no flush: per-system grids and pair lists total ~30 GB"},
+            "phase_ms_rank0": phase,
+            "lanes_mode_systems_per_s_rank0": None if lanes_rate is None else round(lanes_rate, 3),
+            "plain_per_system_systems_per_s_rank0": None if plain_rate is None else round(plain_rate, 3),
+            "packed_over_plain": (None if plain_rate is None else
+                                  round(len(mine) * args.steps / (total_ms / 1e3) / plain_rate, 3)),
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
                            "p99": round(float(np.percentile(lat, 99)), 3)},

@@ -15,6 +15,9 @@
 // iteration i; a system whose check passes leaves the active set.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -496,8 +499,18 @@ int bl_compute(BLState *bl, PackedBatch *pb, const std::vector<int> &sel, int k,
     std::vector<double *> vp;
     std::vector<int> ldp;
     // checks of iteration i for the systems that ran it
+    using Clock = std::chrono::steady_clock;
+    auto ms_since = [](Clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+    };
+    const bool trace = std::getenv("STOKESDT_LANCZOS_TRACE") != nullptr;
+    const Clock::time_point t_start = Clock::now();
+    double t_wait = 0.0, t_solve = 0.0;
     auto check = [&](int i) -> int {
+        Clock::time_point tw = Clock::now();
         BL_CUDA(cudaEventSynchronize(bl->ev[i]));
+        t_wait += ms_since(tw);
+        tw = Clock::now();
         const std::vector<int> &ran = act_at[i];
         parallel_for((int)ran.size(), [&](int j) {
             const int g = ran[j];
@@ -526,15 +539,31 @@ int bl_compute(BLState *bl, PackedBatch *pb, const std::vector<int> &sel, int k,
             x.Dprev = D;
             x.D = std::move(D);
         });
+        t_solve += ms_since(tw);
         for (int g : ran)
             if (ss[g].status != kOk) return bl_error(bl, ss[g].status, "tridiagonal eigensolver did not converge");
         return kOk;
+    };
+    // with the trace on, CUDA events bracket the phases of every iteration
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    auto mark = [&](int phase) -> cudaEvent_t {
+        if (!trace) return nullptr;
+        cudaEvent_t a = nullptr, b2 = nullptr;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b2);
+        cudaEventRecord(a, bl->stream);
+        marks.push_back({phase, {a, b2}});
+        return b2;
+    };
+    auto mark_end = [&](cudaEvent_t e) {
+        if (e) cudaEventRecord(e, bl->stream);
     };
     int it = 0;
     int last_issued = -1;
     for (it = 0; it < bl->max_iters && !act.empty(); it++) {
         act_at[it] = act;
         const int ci = it * k, cw = (it + 1) * k;
+        cudaEvent_t pe = mark(0);
         if (it > 0) {
             st = bl_gemm(bl, (it - 1) * k, k, kBlBt, 0, k, k, 1.0, 0.0, cw);  // W = V_{i-1} B_{i-1}^T
             if (st != kOk) return st;
@@ -551,11 +580,18 @@ int bl_compute(BLState *bl, PackedBatch *pb, const std::vector<int> &sel, int k,
         st = packed_mulvec(pb, (int)act.size(), act.data(), k, 1.0, fp.data(), ldp.data(), it > 0 ? -1.0 : 0.0,
                            vp.data(), ldp.data());
         if (st != kOk) return bl_error(bl, st, "packed product: " + pb->last_error);
+        mark_end(pe);
+        pe = mark(1);
         st = bl_gram(bl, ci, k, cw, k, kBlHistA, it, k);                            // A_i = V_i^T W
         if (st == kOk) st = bl_gemm(bl, ci, k, kBlHistA, it, k, k, -1.0, 1.0, cw);  // W -= V_i A_i
+        mark_end(pe);
+        pe = mark(2);
         if (st == kOk) st = bl_gram(bl, 0, cw, cw, k, kBlCoef, 0, k);               // C = V_{0..i}^T W
         if (st == kOk) st = bl_gemm(bl, 0, cw, kBlCoef, 0, k, k, -1.0, 1.0, cw);    // W -= V_{0..i} C
+        mark_end(pe);
+        pe = mark(3);
         if (st == kOk) st = bl_chol_qr(bl, cw, k, false, it, it);                   // W = V_{i+1} B_i
+        mark_end(pe);
         if (st != kOk) return st;
         BL_CUDA(cudaMemcpy2DAsync(bl->h_hist + (size_t)it * hs, bl->hist_pitch * sizeof(double),
                                   bl->h_sys[0].hist + (size_t)it * hs, bl->mats_stride * sizeof(double),
@@ -596,6 +632,23 @@ int bl_compute(BLState *bl, PackedBatch *pb, const std::vector<int> &sel, int k,
     if (st != kOk) return st;
     // the host copies of the coefficients are read by the queued uploads
     BL_CUDA(cudaStreamSynchronize(bl->stream));
+    if (trace) {
+        double ph[4] = {0, 0, 0, 0};
+        for (auto &m : marks) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, m.second.first, m.second.second);
+            ph[m.first] += t;
+            cudaEventDestroy(m.second.first);
+            cudaEventDestroy(m.second.second);
+        }
+        std::fprintf(stderr, "[batched lanczos] device ms: products %.1f, recurrence %.1f, reorthogonalisation %.1f, "
+                     "QR %.1f\n", ph[0], ph[1], ph[2], ph[3]);
+        std::fprintf(stderr, "[batched lanczos] %zu systems, k %d: %d iterations, %.1f ms total, %.1f ms waiting on the "
+                     "GPU, %.1f ms in host solves; active per iteration:", sel.size(), k, it, ms_since(t_start),
+                     t_wait, t_solve);
+        for (int i = 0; i < it; i++) std::fprintf(stderr, " %zu", act_at[i].size());
+        std::fprintf(stderr, "\n");
+    }
     int out = kOk;
     for (size_t j = 0; j < sel.size(); j++) {
         const SysState &x = ss[sel[j]];

@@ -44,7 +44,9 @@ constexpr int kRowBlockZ = 4;  // z extent of the row blocks of the x passes
 constexpr int kMaxOrder = 8;   // largest supported B-spline order
 constexpr int kTileX = 16;     // kx columns per CTA in the y pass
 constexpr int kTileZ = 8;      // kx columns per CTA in the staged z pass (x 3 components)
-constexpr int kTileZF = 4;     // kx columns per CTA in the register-fused z pass
+// kx columns per CTA in the register-fused z pass: 4 at K = 256 (a 29 KB
+// CTA), 8 below, so smaller grids keep the same bytes in flight per CTA
+__host__ __device__ constexpr int z_fused_tile(int K) { return K <= 128 ? 8 : 4; }
 
 struct SpmeEngine {
     // configuration
@@ -127,8 +129,8 @@ struct SpmeEngine {
     CUtensorMap tmap_z;            // [3*rhs][K z][K y][XS x]
     CUtensorMap tmap_tab0;         // influence tables [K z][K y][XS x] (float)
     CUtensorMap tmap_tab2;
-    CUtensorMap tmap_zf;           // the z map with kTileZF-wide boxes (fused z pass)
-    CUtensorMap tmap_tab0f, tmap_tab2f;  // table maps with kTileZF-wide boxes
+    CUtensorMap tmap_zf;           // the z map with z_fused_tile(K)-wide boxes (fused z pass)
+    CUtensorMap tmap_tab0f, tmap_tab2f;  // table maps with z_fused_tile(K)-wide boxes
     bool tma_tabs = false;         // table maps encoded
     int *d_err = nullptr;          // device error word of the TMA passes (0 = fine)
     // overlapped product: real space and RHS groups of the grid chain on side

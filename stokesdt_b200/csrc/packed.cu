@@ -147,10 +147,10 @@ int packed_create(PackedBatch *pb, const std::vector<SpmeEngine *> &eng, int rhs
         const unsigned by[3] = {(unsigned)kTileX, lines, 1u};
         const unsigned long long dz[4] = {XS, K, K, planes};
         const unsigned long long sz[3] = {XS * el, K * XS * el, K * K * XS * el};
-        const unsigned bzf[4] = {(unsigned)kTileZF, 1u, lines, 1u};
+        const unsigned bzf[4] = {(unsigned)z_fused_tile(c.K), 1u, lines, 1u};
         const unsigned long long dt[4] = {XS, K, K, (unsigned long long)ns};
         const unsigned long long st[3] = {XS * fl, K * XS * fl, K * K * XS * fl};
-        const unsigned bt[4] = {(unsigned)kTileZF, 1u, lines, 1u};
+        const unsigned bt[4] = {(unsigned)z_fused_tile(c.K), 1u, lines, 1u};
         if (!encode_tmap_f2(&c.tmap_y, c.d_grid, 3, dy, sy, by) ||
             !encode_tmap_f2(&c.tmap_zf, c.d_grid, 4, dz, sz, bzf) ||
             !encode_tmap(&c.tmap_tabf, c.d_tab, 4, 4, dt, st, bt))

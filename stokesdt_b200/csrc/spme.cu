@@ -1035,7 +1035,7 @@ __global__ void k_combine(int n3, int nr, int mode, double alpha, double beta, d
 // the influence function and into the inverse transform without a shared-
 // memory round trip: six passes over the tile instead of ten.
 template <int K>
-__host__ __device__ constexpr int kZFusedThreads() { return kTileZF * FftShape<K>::N2; }
+__host__ __device__ constexpr int kZFusedThreads() { return z_fused_tile(K) * FftShape<K>::N2; }
 
 // FWD_ONLY stops after the forward z transform and stores the spectrum (the
 // forward-transform diagnostic sdt_spme_spectrum_device); the product uses
@@ -1051,15 +1051,15 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
 {
     constexpr int H = K / 2;
     constexpr int N1 = FftShape<K>::N1, N2 = FftShape<K>::N2, NR = N1 / N2;
-    constexpr int CS = K * kTileZF;  // float2 per component
-    extern __shared__ __align__(1024) float2 sm[];  // [3][K][kTileZF], then the table tile [K][kTileZF]
+    constexpr int CS = K * z_fused_tile(K);  // float2 per component
+    extern __shared__ __align__(1024) float2 sm[];  // [3][K][z_fused_tile(K)], then the table tile [K][z_fused_tile(K)]
     float *tabs = reinterpret_cast<float *>(sm + 3 * CS);
     __shared__ uint64_t bar;
     // the RHS index runs fastest, so the CTAs that read one influence-table
     // tile run together and share it through L2
     const int r = r0 + blockIdx.x, tx = blockIdx.y, y = blockIdx.z;
     const int tid = threadIdx.x;
-    const int kx0 = tx * kTileZF;
+    const int kx0 = tx * z_fused_tile(K);
     int tabi = 0;
     if constexpr (PACKED) {
         tabi = slot_tab[blockIdx.x / nr_packed];
@@ -1074,12 +1074,12 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
         mbar_arrive_expect_tx(&bar, (uint32_t)(3 * CS * sizeof(float2) + CS * sizeof(float)));
         for (int c = 0; c < 3; c++)
             for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
-                tma_load_4d(sm + c * CS + z0 * kTileZF, &map, &bar, kx0, y, z0, 3 * r + c);
+                tma_load_4d(sm + c * CS + z0 * z_fused_tile(K), &map, &bar, kx0, y, z0, 3 * r + c);
         for (int z0 = 0; z0 < K; z0 += kTmaBoxLines) {
             if constexpr (PACKED)
-                tma_load_4d(tabs + z0 * kTileZF, &tabmap, &bar, kx0, y, z0, tabi);
+                tma_load_4d(tabs + z0 * z_fused_tile(K), &tabmap, &bar, kx0, y, z0, tabi);
             else
-                tma_load_3d(tabs + z0 * kTileZF, &tabmap, &bar, kx0, y, z0);
+                tma_load_3d(tabs + z0 * z_fused_tile(K), &tabmap, &bar, kx0, y, z0);
         }
     }
     const bool ok = mbar_wait(&bar, 0);
@@ -1087,9 +1087,9 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
         if (tid == 0) atomicExch(err, kTmaErrTimeout);
         return;
     }
-    const int col = tid % kTileZF, t = tid / kTileZF;
-    // element e of a column sits at sm[c * CS + e * kTileZF + col]
-    auto at = [&](int c, int e) -> float2 & { return sm[c * CS + e * kTileZF + col]; };
+    const int col = tid % z_fused_tile(K), t = tid / z_fused_tile(K);
+    // element e of a column sits at sm[c * CS + e * z_fused_tile(K) + col]
+    auto at = [&](int c, int e) -> float2 & { return sm[c * CS + e * z_fused_tile(K) + col]; };
 
     // forward step 1 per component: N1-point DFTs of x[N2 j + t], twiddled,
     // stored transposed in place (after every thread has read the component)
@@ -1135,7 +1135,7 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
         if (tid == 0) {
             for (int c2 = 0; c2 < 3; c2++)
                 for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
-                    tma_store_4d(&map, sm + c2 * CS + z0 * kTileZF, kx0, y, z0, 3 * r + c2);
+                    tma_store_4d(&map, sm + c2 * CS + z0 * z_fused_tile(K), kx0, y, z0, 3 * r + c2);
             bulk_commit();
             bulk_wait_read_all();
         }
@@ -1152,7 +1152,7 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
             constexpr int sl = SlotOf<N2, k2>::value;
             const int kz = t + rr * N2 + N1 * k2;
             const float fkz = __ldg(&kmap[kz]);
-            const float m2 = tabs[kz * kTileZF + col];
+            const float m2 = tabs[kz * z_fused_tile(K) + col];
             const float kk = fkx * fkx + fky * fky + fkz * fkz;
             float2 g0 = b[0][rr][sl], g1 = b[1][rr][sl], g2 = b[2][rr][sl];
             if (kk > 0.0f && kx <= H) {
@@ -1219,7 +1219,7 @@ k_zpass_fused_tma(const __grid_constant__ CUtensorMap map, const __grid_constant
     if (tid == 0) {
         for (int c2 = 0; c2 < 3; c2++)
             for (int z0 = 0; z0 < K; z0 += kTmaBoxLines)
-                tma_store_4d(&map, sm + c2 * CS + z0 * kTileZF, kx0, y, z0, 3 * r + c2);
+                tma_store_4d(&map, sm + c2 * CS + z0 * z_fused_tile(K), kx0, y, z0, 3 * r + c2);
         bulk_commit();
         bulk_wait_read_all();
     }
@@ -1243,10 +1243,11 @@ static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *isc
     const size_t smy = (size_t)K * kTileX * sizeof(float2);
     const size_t smz = (size_t)3 * K * kTileZ * sizeof(float2);
     const size_t smz_tma = smz + (size_t)K * kTileZ * sizeof(float);
-    const size_t smzf_tma = (size_t)3 * K * kTileZF * sizeof(float2) + (size_t)K * kTileZF * sizeof(float);
+    constexpr int TZ = z_fused_tile(K);
+    const size_t smzf_tma = (size_t)3 * K * TZ * sizeof(float2) + (size_t)K * TZ * sizeof(float);
     const int ntile = (H + 1 + kTileX - 1) / kTileX;
     const int ntilez = (H + 1 + kTileZ - 1) / kTileZ;
-    const int ntilezf = (H + 1 + kTileZF - 1) / kTileZF;
+    const int ntilezf = (H + 1 + TZ - 1) / TZ;
     SDT_CUDA(cudaFuncSetAttribute(k_spread_xfwd<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     SDT_CUDA(cudaFuncSetAttribute(k_xinv_interp<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     SDT_CUDA(cudaFuncSetAttribute(k_xinv_interp<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
@@ -1422,7 +1423,7 @@ int spme_reserve(SpmeEngine *e, int rhs)
         const unsigned long long dz[4] = {XS, K, K, 3ull * rhs};
         const unsigned long long sz[3] = {XS * el, K * XS * el, K * K * XS * el};
         const unsigned bz[4] = {(unsigned)kTileZ, 1u, lines, 1u};
-        const unsigned bzf[4] = {(unsigned)kTileZF, 1u, lines, 1u};
+        const unsigned bzf[4] = {(unsigned)z_fused_tile(e->K), 1u, lines, 1u};
         e->tma_ready = e->tma_tabs && encode_tmap_f2(&e->tmap_y, e->d_cgrid, 3, dy, sy, by) &&
                        encode_tmap_f2(&e->tmap_z, e->d_cgrid, 4, dz, sz, bz) &&
                        encode_tmap_f2(&e->tmap_zf, e->d_cgrid, 4, dz, sz, bzf);
@@ -1526,7 +1527,7 @@ int spme_create(SpmeEngine *e)
         const unsigned long long dt[3] = {XSl, KK, KK};
         const unsigned long long st[2] = {XSl * el, KK * XSl * el};
         const unsigned bt[3] = {(unsigned)kTileZ, 1u, (unsigned)std::min(K, 256)};
-        const unsigned btf[3] = {(unsigned)kTileZF, 1u, (unsigned)std::min(K, 256)};
+        const unsigned btf[3] = {(unsigned)z_fused_tile(K), 1u, (unsigned)std::min(K, 256)};
         e->tma_tabs = encode_tmap(&e->tmap_tab0, e->d_tab0, 4, 3, dt, st, bt) &&
                       encode_tmap(&e->tmap_tab0f, e->d_tab0, 4, 3, dt, st, btf) &&
                       (e->mono || (encode_tmap(&e->tmap_tab2, e->d_tab2, 4, 3, dt, st, bt) &&
@@ -1878,8 +1879,9 @@ template <int K>
 static int packed_z_k(const PackedClass &c, int nslots, int nr, int *err, cudaStream_t s)
 {
     constexpr int H = K / 2;
-    const size_t smzf = (size_t)3 * K * kTileZF * sizeof(float2) + (size_t)K * kTileZF * sizeof(float);
-    const int ntilezf = (H + 1 + kTileZF - 1) / kTileZF;
+    constexpr int TZ = z_fused_tile(K);
+    const size_t smzf = (size_t)3 * K * TZ * sizeof(float2) + (size_t)K * TZ * sizeof(float);
+    const int ntilezf = (H + 1 + TZ - 1) / TZ;
     auto kern = k_zpass_fused_tma<K, false, true>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smzf) != cudaSuccess)
         return kErrCuda;

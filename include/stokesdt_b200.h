@@ -21,6 +21,11 @@
  *                          (BrwnBase::Compute src/brwn/brwn_base.h:44-46)
  *   sdt_lanczos_destroy    BrwnLanczos::~BrwnLanczos           src/brwn/brwn_lanczos.cc:217-221
  *   sdt_bd_advance         BDSimBox::Advance step loop         src/simbox/simbox_bd.cc:296-366
+ *   sdt_ewald_create       MobEwald::MobEwald + MobEwald::Init src/mob/mob_ewald.cc:21-108
+ *   sdt_ewald_update       MobEwald::Update (EwaldKernel)      src/mob/mob_ewald.cc:111-127,
+ *                          src/mob/ewald.cc:86-330 (tables :643-797)
+ *   sdt_ewald_mulvec       MobEwald::MulVector                 src/mob/mob_ewald.cc:131-152
+ *   sdt_ewald_get_matrix   MobEwald::GetMatrix                 src/mob/mob_ewald.cc:155-165
  *   sdt_steric_create      StericForce::StericForce + Init     src/force/force_steric.cc:54-88
  *   sdt_steric_accumulate  StericForce::Accumulate (ForceBase)  src/force/force_steric.cc:91-104,
  *                          src/force/force_base.h:55-65 (PairListS src/pairlist/pair_s.cc:99-186)
@@ -136,6 +141,38 @@ const char *sdt_spme_last_error(const sdt_spme *h);
 
 void sdt_spme_destroy(sdt_spme *h);
 
+/* ---- Dense Ewald RPY mobility (MobEwald) ---- */
+
+typedef struct sdt_ewald sdt_ewald;
+
+/* The 3N x 3N Ewald-summed RPY mobility matrix of npos particles with radii
+ * rdi (copied) in a cube of edge box_size, FP64, held on the device (the
+ * small-N counterpart of the SPME engine).  tol sets the real- and
+ * reciprocal-space cut-offs by the reference's rules; xi <= 0 selects the
+ * reference's default 10^(1/6) sqrt(pi) / L.  SDT_ERR_ALLOC when the matrix
+ * (72 N^2 bytes) does not fit in half the free device memory. */
+int sdt_ewald_create(int npos, const double *rdi, double box_size, double tol, double xi, int device,
+                     sdt_ewald **out);
+/* Builds the matrix at positions pos[3*npos] (host; synchronous) or d_pos
+ * (device; asynchronous on the engine stream). */
+int sdt_ewald_update(sdt_ewald *h, const double *pos);
+int sdt_ewald_update_device(sdt_ewald *h, const double *d_pos);
+/* v := alpha M f + beta v for nrhs vectors (beta == 0 ignores v); host
+ * pointers (synchronous) or device pointers (asynchronous). */
+int sdt_ewald_mulvec(sdt_ewald *h, int nrhs, double alpha, int ldf, const double *f, double beta, int ldv,
+                     double *v);
+int sdt_ewald_mulvec_device(sdt_ewald *h, int nrhs, double alpha, int ldf, const double *d_f, double beta,
+                            int ldv, double *d_v);
+/* Copies the matrix (row-major, leading dimension ldm >= 3 npos) to the host. */
+int sdt_ewald_get_matrix(sdt_ewald *h, int ldm, double *mat);
+/* xi, the cut-offs and the numbers of real-space images and reciprocal vectors
+ * (any pointer may be NULL). */
+int sdt_ewald_info(const sdt_ewald *h, double *xi, double *rmax, double *kmax, int *nimages, int *nkvectors);
+int sdt_ewald_dim(const sdt_ewald *h);
+int sdt_ewald_set_stream(sdt_ewald *h, void *stream);
+const char *sdt_ewald_last_error(const sdt_ewald *h);
+void sdt_ewald_destroy(sdt_ewald *h);
+
 /* ---- Block Lanczos sqrt(M) z (BrwnLanczos) ---- */
 
 /* dim = 3*npos; max_nrhs is clamped to dim/3 as in BrwnLanczos::Init
@@ -156,6 +193,14 @@ int sdt_lanczos_compute(sdt_lanczos *h, sdt_spme *mob, int nrhs, int ldz, const 
 /* Same with device pointers for z and y (synchronous return of iters). */
 int sdt_lanczos_compute_device(sdt_lanczos *h, sdt_spme *mob, int nrhs, int ldz,
                                const double *d_z, int ldy, double *d_y, int *iters);
+
+/* sdt_lanczos_compute / _device with the dense Ewald mobility
+ * (BrwnLanczos::Compute on MobEwald, as tests/lanczos/testlanczos.cc of the
+ * reference does). */
+int sdt_lanczos_compute_ewald(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz, const double *z, int ldy,
+                              double *y, int *iters);
+int sdt_lanczos_compute_ewald_device(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz, const double *d_z,
+                                     int ldy, double *d_y, int *iters);
 
 /* Bind the solver to an existing cudaStream_t (NULL = its own).  The
  * mobility products it requests run on this stream too. */

@@ -7,6 +7,7 @@
  * libstokesdt_b200.so.
  *
  *   MobSpmeGpu     : MobBase   replaces MobSpme      (src/mob/mob_spme.h:21-125)
+ *   MobEwaldGpu    : MobBase   replaces MobEwald     (src/mob/mob_ewald.h)
  *   BrwnLanczosGpu : BrwnBase  replaces BrwnLanczos  (src/brwn/brwn_lanczos.h:20-110)
  *   StericForceGpu : ForceBase replaces StericForce  (src/force/force_steric.h:20-86);
  *                    defined when force_base.h has been included first (the
@@ -94,6 +95,57 @@ class MobSpmeGpu : public MobBase {
     sdt_spme *h_;
 };
 
+class MobEwaldGpu : public MobBase {
+  public:
+    MobEwaldGpu(const int npos, const double *rdi, const double box_size, const double tol, const double xi = 0.0,
+                const int device = 0)
+        : npos_(npos), rdi_(rdi, rdi + npos), box_size_(box_size), tol_(tol), xi_(xi), device_(device), h_(0)
+    {
+    }
+
+    virtual ~MobEwaldGpu() { sdt_ewald_destroy(h_); }
+
+    virtual bool Init()
+    {
+        if (npos_ <= 0) return false;
+        return sdt_ewald_create(npos_, &rdi_[0], box_size_, tol_, xi_, device_, &h_) == SDT_OK;
+    }
+
+    virtual void Update(const double *pos, const double * /*rdi: fixed at construction*/)
+    {
+        Report(sdt_ewald_update(h_, pos), "Update");
+    }
+
+    virtual void MulVector(const int num_rhs, const double alpha, const int ldf, const double *f,
+                           const double beta, const int ldv, double *v)
+    {
+        Report(sdt_ewald_mulvec(h_, num_rhs, alpha, ldf, f, beta, ldv, v), "MulVector");
+    }
+
+    void GetMatrix(const int ldm, double *mat) { Report(sdt_ewald_get_matrix(h_, ldm, mat), "GetMatrix"); }
+
+    virtual int dim() { return 3 * npos_; }
+
+    sdt_ewald *handle() { return h_; }
+
+  private:
+    void Report(int st, const char *what)
+    {
+        if (st != SDT_OK)
+            fprintf(stderr, "ERROR: MobEwaldGpu::%s: status %d: %s\n", what, st,
+                    h_ ? sdt_ewald_last_error(h_) : "not initialised");
+    }
+
+    MobEwaldGpu(const MobEwaldGpu &);
+    void operator=(const MobEwaldGpu &);
+
+    int npos_;
+    std::vector<double> rdi_;
+    double box_size_, tol_, xi_;
+    int device_;
+    sdt_ewald *h_;
+};
+
 class BrwnLanczosGpu : public BrwnBase {
   public:
     BrwnLanczosGpu(const int dim, const int max_iters, const int max_nrhs, const double tol,
@@ -109,18 +161,21 @@ class BrwnLanczosGpu : public BrwnBase {
         return sdt_lanczos_create(dim_, max_iters_, max_nrhs_, tol_, device_, &h_) == SDT_OK;
     }
 
-    /* mob must be a MobSpmeGpu (the products run on its GPU engine). */
+    /* mob must be a MobSpmeGpu or a MobEwaldGpu (the products run on its
+     * GPU engine). */
     virtual void Compute(MobBase *mob, const int num_rhs, const int ldz, const double *z,
                          const int ldy, double *y)
     {
         MobSpmeGpu *g = dynamic_cast<MobSpmeGpu *>(mob);
-        if (g == 0) {
-            fprintf(stderr, "ERROR: BrwnLanczosGpu::Compute needs a MobSpmeGpu\n");
+        MobEwaldGpu *ew = dynamic_cast<MobEwaldGpu *>(mob);
+        if (g == 0 && ew == 0) {
+            fprintf(stderr, "ERROR: BrwnLanczosGpu::Compute needs a MobSpmeGpu or a MobEwaldGpu\n");
             return;
         }
         int groups = (num_rhs + max_nrhs_ - 1) / max_nrhs_;
         std::vector<int> iters(groups > 0 ? groups : 1, 0);
-        const int st = sdt_lanczos_compute(h_, g->handle(), num_rhs, ldz, z, ldy, y, &iters[0]);
+        const int st = g ? sdt_lanczos_compute(h_, g->handle(), num_rhs, ldz, z, ldy, y, &iters[0])
+                         : sdt_lanczos_compute_ewald(h_, ew->handle(), num_rhs, ldz, z, ldy, y, &iters[0]);
         if (st == SDT_ERR_NOT_CONVERGED)
             fprintf(stderr, "WARNING: BrwnLanczosGpu: NOT converged\n");
         else if (st != SDT_OK)

@@ -29,7 +29,7 @@ import os
 
 import numpy as np
 
-__all__ = ["MobSpme", "BrwnLanczos", "lib", "LIB_PATH", "StokesError", "MODE_FULL", "MODE_REAL",
+__all__ = ["MobSpme", "MobEwald", "BrwnLanczos", "lib", "LIB_PATH", "StokesError", "MODE_FULL", "MODE_REAL",
            "MODE_RECIP"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -90,6 +90,25 @@ SIGNATURES = {
     "sdt_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong), _ip]),
     "sdt_batch_synchronize": (ctypes.c_int, [_vp]),
     "sdt_batch_set_packed": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "sdt_ewald_create": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_int, ctypes.POINTER(_vp)]),
+    "sdt_ewald_update": (ctypes.c_int, [_vp, _dp]),
+    "sdt_ewald_update_device": (ctypes.c_int, [_vp, _vp]),
+    "sdt_ewald_mulvec": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, ctypes.c_double,
+                                        ctypes.c_int, _dp]),
+    "sdt_ewald_mulvec_device": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp,
+                                               ctypes.c_double, ctypes.c_int, _vp]),
+    "sdt_ewald_get_matrix": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "sdt_ewald_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), _ip, _ip]),
+    "sdt_ewald_dim": (ctypes.c_int, [_vp]),
+    "sdt_ewald_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "sdt_ewald_last_error": (ctypes.c_char_p, [_vp]),
+    "sdt_ewald_destroy": (None, [_vp]),
+    "sdt_lanczos_compute_ewald": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                                 _ip]),
+    "sdt_lanczos_compute_ewald_device": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                        _vp, _ip]),
     "sdt_batch_get_packed": (ctypes.c_int, [_vp]),
     "sdt_batch_last_error": (ctypes.c_char_p, [_vp]),
     "sdt_batch_destroy": (None, [_vp]),
@@ -310,6 +329,92 @@ class MobSpme:
             pass
 
 
+class MobEwald:
+    """Dense Ewald RPY mobility matrix on one GPU, FP64 (drop-in for the
+    reference's MobEwald, src/mob/mob_ewald.h: Init / Update / MulVector /
+    GetMatrix / dim).  xi = None selects the reference's default
+    10^(1/6) sqrt(pi) / L."""
+
+    def __init__(self, npos, rdi, box_size, tol, xi=None, device=0):
+        self.npos = int(npos)
+        self.rdi = _f64(rdi).reshape(-1).copy()
+        if self.rdi.size != self.npos:
+            raise ValueError("rdi must have npos entries")
+        self.box_size = float(box_size)
+        self.tol = float(tol)
+        self.xi = 0.0 if xi is None else float(xi)
+        self.device = int(device)
+        self._h = None
+        self.last_error = ""
+
+    def Init(self) -> bool:
+        h = _vp()
+        st = lib().sdt_ewald_create(self.npos, _ptr(self.rdi), self.box_size, self.tol, self.xi, self.device,
+                                    ctypes.byref(h))
+        if st != 0:
+            self.last_error = STATUS.get(st, str(st))
+            return False
+        self._h = h
+        return True
+
+    def _check(self, st):
+        if st != 0:
+            msg = lib().sdt_ewald_last_error(self._h).decode() if self._h else ""
+            raise StokesError(st, msg)
+
+    def _need(self):
+        if self._h is None:
+            raise StokesError(-4, "Init() has not succeeded")
+
+    def Update(self, pos, rdi=None):
+        self._need()
+        pos = _f64(pos).reshape(-1)
+        if pos.size < 3 * self.npos:
+            raise ValueError("pos must hold 3*npos values")
+        self._check(lib().sdt_ewald_update(self._h, _ptr(pos)))
+
+    def MulVector(self, num_rhs, alpha, ldf, f, beta, ldv, v):
+        """v := alpha*M*f + beta*v (in place on v)."""
+        self._need()
+        f = _f64(f)
+        if not isinstance(v, np.ndarray) or v.dtype != np.float64 or not v.flags["C_CONTIGUOUS"]:
+            raise TypeError("v must be a C-contiguous float64 numpy array (updated in place)")
+        self._check(lib().sdt_ewald_mulvec(self._h, int(num_rhs), float(alpha), int(ldf), _ptr(f), float(beta),
+                                           int(ldv), _ptr(v)))
+
+    def GetMatrix(self):
+        self._need()
+        n = 3 * self.npos
+        m = np.zeros((n, n))
+        self._check(lib().sdt_ewald_get_matrix(self._h, n, _ptr(m)))
+        return m
+
+    def info(self) -> dict:
+        xi, rmax, kmax = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        nr, nk = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().sdt_ewald_info(self._h, ctypes.byref(xi), ctypes.byref(rmax), ctypes.byref(kmax),
+                                         ctypes.byref(nr), ctypes.byref(nk)))
+        return {"xi": xi.value, "rmax": rmax.value, "kmax": kmax.value, "nimages": nr.value, "nk": nk.value}
+
+    def dim(self) -> int:
+        return 3 * self.npos
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h is not None:
+            lib().sdt_ewald_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class StericForce:
     """Steric force on one GPU (drop-in for the reference's StericForce,
     src/force/force_steric.h: ForceBase::Init / Accumulate / Compute)."""
@@ -407,8 +512,8 @@ class BrwnLanczos:
             raise TypeError("y must be a C-contiguous float64 numpy array (updated in place)")
         ngroups = max(1, (int(num_rhs) + self.max_nrhs - 1) // self.max_nrhs)
         iters = (ctypes.c_int * ngroups)()
-        st = lib().sdt_lanczos_compute(self._h, mob.handle, int(num_rhs), int(ldz), _ptr(z), int(ldy),
-                                       _ptr(y), iters)
+        compute = lib().sdt_lanczos_compute_ewald if isinstance(mob, MobEwald) else lib().sdt_lanczos_compute
+        st = compute(self._h, mob.handle, int(num_rhs), int(ldz), _ptr(z), int(ldy), _ptr(y), iters)
         self.last_iters = list(iters)
         if st not in (0, -5):
             raise StokesError(st, lib().sdt_lanczos_last_error(self._h).decode())

@@ -12,7 +12,9 @@
 
 namespace {
 
-int fail(sdt::SpmeEngine *e, int st, const std::string &msg)
+// Records msg as the engine's last error (any engine with a last_error).
+template <typename Engine>
+int fail(Engine *e, int st, const std::string &msg)
 {
     e->last_error = msg;
     return st;
@@ -725,6 +727,224 @@ int sdt_lanczos_compute_device(sdt_lanczos *h, sdt_spme *mob, int nrhs, int ldz,
     if (st != SDT_OK && st != SDT_ERR_NOT_CONVERGED) return st;
     if (cudaStreamSynchronize(h->s.stream) != cudaSuccess) {
         h->s.last_error = "stream synchronize failed";
+        return SDT_ERR_CUDA;
+    }
+    return st;
+}
+
+// ---- dense Ewald (MobEwald) ----
+
+int sdt_ewald_create(int npos, const double *rdi, double box_size, double tol, double xi, int device,
+                     sdt_ewald **out)
+{
+    if (!out || !rdi) return SDT_ERR_INVALID;
+    *out = nullptr;
+    sdt_ewald *h = new (std::nothrow) sdt_ewald;
+    if (!h) return SDT_ERR_ALLOC;
+    sdt::EwaldEngine *e = &h->e;
+    e->device = device;
+    e->npos = npos;
+    e->box = box_size;
+    e->tol = tol;
+    e->xi = xi;
+    const int st = sdt::ewald_create(e, rdi);
+    if (st != SDT_OK) {
+        sdt::ewald_free(e);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return SDT_OK;
+}
+
+int sdt_ewald_update_device(sdt_ewald *h, const double *d_pos)
+{
+    if (!h || !d_pos) return SDT_ERR_INVALID;
+    CAPI_CUDA(&h->e, cudaSetDevice(h->e.device));
+    return sdt::ewald_update(&h->e, d_pos);
+}
+
+int sdt_ewald_update(sdt_ewald *h, const double *pos)
+{
+    if (!h || !pos) return SDT_ERR_INVALID;
+    sdt::EwaldEngine *e = &h->e;
+    CAPI_CUDA(e, cudaSetDevice(e->device));
+    CAPI_CUDA(e, cudaMemcpyAsync(e->d_pos, pos, (size_t)e->n3 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    const int st = sdt::ewald_update(e, e->d_pos);
+    if (st != SDT_OK) return st;
+    CAPI_CUDA(e, cudaStreamSynchronize(e->stream));
+    return SDT_OK;
+}
+
+int sdt_ewald_mulvec_device(sdt_ewald *h, int nrhs, double alpha, int ldf, const double *d_f, double beta, int ldv,
+                            double *d_v)
+{
+    if (!h || !d_f || !d_v) return SDT_ERR_INVALID;
+    CAPI_CUDA(&h->e, cudaSetDevice(h->e.device));
+    return sdt::ewald_mulvec(&h->e, nrhs, alpha, ldf, d_f, beta, ldv, d_v);
+}
+
+int sdt_ewald_mulvec(sdt_ewald *h, int nrhs, double alpha, int ldf, const double *f, double beta, int ldv, double *v)
+{
+    if (!h || !f || !v || nrhs < 0) return SDT_ERR_INVALID;
+    sdt::EwaldEngine *e = &h->e;
+    if (ldf < e->n3 || ldv < e->n3) {
+        e->last_error = "leading dimensions must be >= 3*npos";
+        return SDT_ERR_INVALID;
+    }
+    if (nrhs == 0) return SDT_OK;
+    CAPI_CUDA(e, cudaSetDevice(e->device));
+    if (nrhs > e->host_cap) {
+        cudaFree(e->d_fin);
+        cudaFree(e->d_vout);
+        e->d_fin = e->d_vout = nullptr;
+        e->host_cap = 0;
+        const size_t bytes = (size_t)nrhs * e->n3 * sizeof(double);
+        if (cudaMalloc(&e->d_fin, bytes) != cudaSuccess || cudaMalloc(&e->d_vout, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            e->last_error = "device allocation of the staging buffers failed";
+            return SDT_ERR_ALLOC;
+        }
+        e->host_cap = nrhs;
+    }
+    const size_t row = (size_t)e->n3 * sizeof(double);
+    CAPI_CUDA(e, cudaMemcpy2DAsync(e->d_fin, row, f, (size_t)ldf * sizeof(double), row, nrhs, cudaMemcpyHostToDevice,
+                                   e->stream));
+    if (beta != 0.0)
+        CAPI_CUDA(e, cudaMemcpy2DAsync(e->d_vout, row, v, (size_t)ldv * sizeof(double), row, nrhs,
+                                       cudaMemcpyHostToDevice, e->stream));
+    const int st = sdt::ewald_mulvec(e, nrhs, alpha, e->n3, e->d_fin, beta, e->n3, e->d_vout);
+    if (st != SDT_OK) return st;
+    CAPI_CUDA(e, cudaMemcpy2DAsync(v, (size_t)ldv * sizeof(double), e->d_vout, row, row, nrhs, cudaMemcpyDeviceToHost,
+                                   e->stream));
+    CAPI_CUDA(e, cudaStreamSynchronize(e->stream));
+    return SDT_OK;
+}
+
+int sdt_ewald_get_matrix(sdt_ewald *h, int ldm, double *mat)
+{
+    if (!h || !mat) return SDT_ERR_INVALID;
+    sdt::EwaldEngine *e = &h->e;
+    if (ldm < e->n3) {
+        e->last_error = "ldm must be >= 3*npos";
+        return SDT_ERR_INVALID;
+    }
+    if (!e->updated) {
+        e->last_error = "Update() must be called first";
+        return SDT_ERR_STATE;
+    }
+    CAPI_CUDA(e, cudaSetDevice(e->device));
+    CAPI_CUDA(e, cudaMemcpy2DAsync(mat, (size_t)ldm * sizeof(double), e->d_mat, (size_t)e->ldm * sizeof(double),
+                                   (size_t)e->n3 * sizeof(double), e->n3, cudaMemcpyDeviceToHost, e->stream));
+    CAPI_CUDA(e, cudaStreamSynchronize(e->stream));
+    return SDT_OK;
+}
+
+int sdt_ewald_info(const sdt_ewald *h, double *xi, double *rmax, double *kmax, int *nimages, int *nkvectors)
+{
+    if (!h) return SDT_ERR_INVALID;
+    if (xi) *xi = h->e.xi;
+    if (rmax) *rmax = h->e.rmax;
+    if (kmax) *kmax = h->e.kmax;
+    if (nimages) *nimages = h->e.nr;
+    if (nkvectors) *nkvectors = h->e.nk;
+    return SDT_OK;
+}
+
+int sdt_ewald_dim(const sdt_ewald *h) { return h ? h->e.n3 : SDT_ERR_INVALID; }
+
+int sdt_ewald_set_stream(sdt_ewald *h, void *stream)
+{
+    if (!h) return SDT_ERR_INVALID;
+    sdt::EwaldEngine *e = &h->e;
+    CAPI_CUDA(e, cudaStreamSynchronize(e->stream));
+    if (e->own_stream) cudaStreamDestroy(e->stream);
+    e->own_stream = false;
+    e->stream = static_cast<cudaStream_t>(stream);
+    if (!e->stream) {
+        CAPI_CUDA(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        e->own_stream = true;
+    }
+    return SDT_OK;
+}
+
+const char *sdt_ewald_last_error(const sdt_ewald *h) { return h ? h->e.last_error.c_str() : "null handle"; }
+
+void sdt_ewald_destroy(sdt_ewald *h)
+{
+    if (!h) return;
+    sdt::ewald_free(&h->e);
+    delete h;
+}
+
+namespace {
+sdt::MobOp ewald_op(sdt::EwaldEngine *e)
+{
+    sdt::MobOp op;
+    op.dim = e->n3;
+    op.mulvec = [e](int nr, double a, int ldf, const double *f, double b, int ldv, double *v, cudaStream_t s) {
+        cudaStream_t saved = e->stream;
+        e->stream = s;
+        const int st = sdt::ewald_mulvec(e, nr, a, ldf, f, b, ldv, v);
+        e->stream = saved;
+        return st;
+    };
+    op.error = [e]() { return e->last_error; };
+    return op;
+}
+}  // namespace
+
+int sdt_lanczos_compute_ewald_device(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz, const double *d_z, int ldy,
+                                     double *d_y, int *iters)
+{
+    if (!h || !mob || !d_z || !d_y) return SDT_ERR_INVALID;
+    sdt::LanczosState *lz = &h->s;
+    if (cudaSetDevice(lz->device) != cudaSuccess) return SDT_ERR_CUDA;
+    // the matrix is built on the engine stream: the solver's stream waits for it
+    if (cudaStreamSynchronize(mob->e.stream) != cudaSuccess) return SDT_ERR_CUDA;
+    const int st = sdt::lanczos_compute_op(lz, ewald_op(&mob->e), nrhs, ldz, d_z, ldy, d_y, iters);
+    if (cudaStreamSynchronize(lz->stream) != cudaSuccess) return SDT_ERR_CUDA;
+    return st;
+}
+
+int sdt_lanczos_compute_ewald(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz, const double *z, int ldy,
+                              double *y, int *iters)
+{
+    if (!h || !mob || !z || !y) return SDT_ERR_INVALID;
+    sdt::LanczosState *lz = &h->s;
+    if (nrhs < 0 || ldz < lz->dim || ldy < lz->dim) {
+        lz->last_error = "bad nrhs or leading dimension";
+        return SDT_ERR_INVALID;
+    }
+    if (nrhs == 0) return SDT_OK;
+    if (cudaSetDevice(lz->device) != cudaSuccess) return SDT_ERR_CUDA;
+    const int n = lz->dim;
+    if (nrhs > lz->host_cap) {
+        cudaFree(lz->d_zin);
+        cudaFree(lz->d_yout);
+        lz->d_zin = lz->d_yout = nullptr;
+        lz->host_cap = 0;
+        const size_t bytes = (size_t)nrhs * n * sizeof(double);
+        if (cudaMalloc(&lz->d_zin, bytes) != cudaSuccess || cudaMalloc(&lz->d_yout, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            lz->last_error = "device allocation of staging buffers failed";
+            return SDT_ERR_ALLOC;
+        }
+        lz->host_cap = nrhs;
+    }
+    const size_t row = (size_t)n * sizeof(double);
+    if (cudaMemcpy2DAsync(lz->d_zin, row, z, (size_t)ldz * sizeof(double), row, nrhs, cudaMemcpyHostToDevice,
+                          lz->stream) != cudaSuccess) {
+        lz->last_error = "copy of z failed";
+        return SDT_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(mob->e.stream) != cudaSuccess) return SDT_ERR_CUDA;
+    const int st = sdt::lanczos_compute_op(lz, ewald_op(&mob->e), nrhs, n, lz->d_zin, n, lz->d_yout, iters);
+    if (st != SDT_OK && st != SDT_ERR_NOT_CONVERGED) return st;
+    if (cudaMemcpy2DAsync(y, (size_t)ldy * sizeof(double), lz->d_yout, row, row, nrhs, cudaMemcpyDeviceToHost,
+                          lz->stream) != cudaSuccess ||
+        cudaStreamSynchronize(lz->stream) != cudaSuccess) {
+        lz->last_error = "copy of y failed";
         return SDT_ERR_CUDA;
     }
     return st;

@@ -6,6 +6,7 @@
 #include "bd.h"
 #include "batch.h"
 #include "serve.h"
+#include "ewald.h"
 
 struct sdt_spme {
     sdt::SpmeEngine e;
@@ -29,4 +30,8 @@ struct sdt_batch {
 
 struct sdt_serve {
     sdt::ServeState s;
+};
+
+struct sdt_ewald {
+    sdt::EwaldEngine e;
 };

@@ -696,7 +696,7 @@ struct PhaseTimer {
     }
 };
 
-static int block_lanczos(LanczosState *lz, SpmeEngine *mob, int k, int ldz, const double *d_z, int ldy,
+static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, const double *d_z, int ldy,
                          double *d_y, int *iters_out)
 {
     const int n = lz->dim, ldv = lz->ldv, hs = lz->hist_stride, kk = k * k;
@@ -889,14 +889,14 @@ static int block_lanczos(LanczosState *lz, SpmeEngine *mob, int k, int ldz, cons
             // W = V_{i-1} B_{i-1}^T, then W = M V_i - W
             st = block_gemm(lz, k, blk(it - 1), ldv, Bt, k, 0.0, W, ldv);
             if (st != kOk) break;
-            st = spme_mulvec(mob, 0, k, 1.0, ldv, Vi, -1.0, ldv, W);
+            st = mob.mulvec(k, 1.0, ldv, Vi, -1.0, ldv, W, lz->stream);
         } else {
-            st = spme_mulvec(mob, 0, k, 1.0, ldv, Vi, 0.0, ldv, W);
+            st = mob.mulvec(k, 1.0, ldv, Vi, 0.0, ldv, W, lz->stream);
         }
         lz->products++;
         pt.end();
         if (st != kOk) {
-            lz->last_error = "mobility product failed: " + mob->last_error;
+            lz->last_error = "mobility product failed: " + mob.error();
             break;
         }
         // A_i = V_i^T W ; W -= V_i A_i
@@ -958,7 +958,24 @@ static int block_lanczos(LanczosState *lz, SpmeEngine *mob, int k, int ldz, cons
 int lanczos_compute(LanczosState *lz, SpmeEngine *mob, int nrhs, int ldz, const double *d_z, int ldy,
                     double *d_y, int *iters)
 {
-    if (mob->npos * 3 != lz->dim) {
+    MobOp op;
+    op.dim = 3 * mob->npos;
+    // the mobility products run on the solver's stream, ordered after its work
+    op.mulvec = [mob](int nr, double a, int ldf, const double *f, double b, int ldv, double *v, cudaStream_t s) {
+        cudaStream_t saved = mob->stream;
+        mob->stream = s;
+        const int st = spme_mulvec(mob, 0, nr, a, ldf, f, b, ldv, v);
+        mob->stream = saved;
+        return st;
+    };
+    op.error = [mob]() { return mob->last_error; };
+    return lanczos_compute_op(lz, op, nrhs, ldz, d_z, ldy, d_y, iters);
+}
+
+int lanczos_compute_op(LanczosState *lz, const MobOp &mob, int nrhs, int ldz, const double *d_z, int ldy,
+                       double *d_y, int *iters)
+{
+    if (mob.dim != lz->dim) {
         lz->last_error = "mobility dimension does not match the Lanczos dimension";
         return kErrInvalid;
     }
@@ -969,23 +986,16 @@ int lanczos_compute(LanczosState *lz, SpmeEngine *mob, int nrhs, int ldz, const 
     const Clock::time_point t_start = Clock::now();
     lz->t_sync_ms = lz->t_eigen_ms = lz->t_wait_ms = 0.0;
     lz->products = 0;
-    // the mobility products run on the engine stream; order them after ours
-    cudaStream_t saved = mob->stream;
-    mob->stream = lz->stream;
     int status = kOk;
     int g = 0;
     for (int r0 = 0; r0 < nrhs; r0 += lz->max_nrhs, g++) {
         const int k = std::min(lz->max_nrhs, nrhs - r0);
         int it = -1;
         const int st = block_lanczos(lz, mob, k, ldz, d_z + (size_t)r0 * ldz, ldy, d_y + (size_t)r0 * ldy, &it);
-        if (st != kOk) {
-            mob->stream = saved;
-            return st;
-        }
+        if (st != kOk) return st;
         if (iters) iters[g] = it;
         if (it < 0) status = kErrNotConverged;
     }
-    mob->stream = saved;
     if (std::getenv("STOKESDT_LANCZOS_TRACE"))
         fprintf(stderr, "[lanczos] %d RHS: total %.1f ms, waiting on GPU %.1f ms, eigensolves %.1f ms "
                 "(blocked on them %.1f ms), %lld block products\n", nrhs, ms_since(t_start), lz->t_sync_ms,

@@ -1,6 +1,7 @@
 // Internal state of one block-Lanczos solver (BrwnLanczos) on one GPU.
 #pragma once
 #include <cuda_runtime.h>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -45,9 +46,22 @@ struct LanczosState {
     std::string last_error;
 };
 
+// A mobility operator the solver applies: v := alpha M f + beta v for nrhs
+// device vectors, queued on stream s (the SPME engine or the dense Ewald).
+struct MobOp {
+    int dim = 0;
+    std::function<int(int nrhs, double alpha, int ldf, const double *f, double beta, int ldv, double *v,
+                      cudaStream_t s)>
+        mulvec;
+    std::function<std::string()> error;
+};
+
 int lanczos_alloc(LanczosState *lz);
 void lanczos_free(LanczosState *lz);
 int lanczos_compute(LanczosState *lz, SpmeEngine *mob, int nrhs, int ldz, const double *d_z, int ldy,
                     double *d_y, int *iters);
+// The same on any mobility operator.
+int lanczos_compute_op(LanczosState *lz, const MobOp &mob, int nrhs, int ldz, const double *d_z, int ldy,
+                       double *d_y, int *iters);
 
 }  // namespace sdt

@@ -15,7 +15,9 @@
  *          tol; pos[3N], rdi[N], f[nrhs][3N], z[nrhs][3N]
  * out.bin: v_full, v_real, v_recip [nrhs][3N] (v := alpha M f + beta f, as
  *          testspme.cc starts v from f), y1[3N] (1 RHS), y[nrhs][3N] (nrhs
- *          RHS) of BrwnLanczosGpu::Compute (max_iters 100, max_nrhs 16)
+ *          RHS) of BrwnLanczosGpu::Compute (max_iters 100, max_nrhs 16),
+ *          v_ewald [nrhs][3N] from MobEwaldGpu (tol 1e-12, default xi) as
+ *          testspme.cc's MobEwald
  */
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +28,7 @@
 
 using stokesdt::BrwnBase;
 using stokesdt::BrwnLanczosGpu;
+using stokesdt::MobEwaldGpu;
 using stokesdt::MobBase;
 using stokesdt::MobSpmeGpu;
 
@@ -75,6 +78,17 @@ int main(int argc, char **argv)
     brwn->Compute(mob, 1, ldm, &z[0], ldm, &y1[0]);
     brwn->Compute(mob, nrhs, ldm, &z[0], ldm, &y[0]);
 
+    // testspme.cc:110-113, 127: the dense Ewald product through MobBase
+    MobEwaldGpu *ewald = new MobEwaldGpu(npos, &rdi[0], box, 1.0e-12);
+    MobBase *mob_ewald = ewald;
+    if (!mob_ewald->Init()) {
+        fprintf(stderr, "MobEwaldGpu::Init failed\n");
+        return 1;
+    }
+    mob_ewald->Update(&pos[0], &rdi[0]);
+    std::vector<double> v_ewald(f);
+    mob_ewald->MulVector(nrhs, alpha, ldm, &f[0], beta, ldm, &v_ewald[0]);
+
     FILE *fo = fopen(argv[2], "wb");
     if (!fo) return 2;
     fwrite(&v_full[0], sizeof(double), v_full.size(), fo);
@@ -82,7 +96,9 @@ int main(int argc, char **argv)
     fwrite(&v_recip[0], sizeof(double), v_recip.size(), fo);
     fwrite(&y1[0], sizeof(double), y1.size(), fo);
     fwrite(&y[0], sizeof(double), y.size(), fo);
+    fwrite(&v_ewald[0], sizeof(double), v_ewald.size(), fo);
     fclose(fo);
+    delete ewald;
     delete brwn;
     delete spme;
     return 0;

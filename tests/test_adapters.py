@@ -19,6 +19,8 @@ int main()
 {
     double rdi[3] = {1.0, 1.0, 1.0};
     stokesdt::MobSpmeGpu m(3, rdi, 10.0, 0.5, 3.0, 32, 6);
+    stokesdt::MobEwaldGpu ew(3, rdi, 10.0, 1e-12);
+    if (ew.dim() != 9) return 1;
     stokesdt::BrwnLanczosGpu b(9, 10, 2, 1e-6);
     stokesdt::StericForceGpu s(3, rdi, 10.0, 2.0, 125.0);
     stokesdt::MobBase *base = &m;

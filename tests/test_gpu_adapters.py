@@ -7,8 +7,9 @@ built against the reference headers by tests/adapter_build.py).
 
 Inputs and expected outputs are the committed golden vectors of the
 reference's N1000_Phi0.1.xyz case: MobSpme and dense MobEwald products
-(3 RHS, alpha 2.1, beta 1.1; bar 1e-6) and the dense symmetric square root of
-the Ewald matrix applied to the Lanczos vectors (bar 1e-5)."""
+(3 RHS, alpha 2.1, beta 1.1; bar 1e-6, and 1e-10 for MobEwaldGpu, FP64) and
+the dense symmetric square root of the Ewald matrix applied to the Lanczos
+vectors (bar 1e-5)."""
 import os
 import subprocess
 import tempfile
@@ -36,9 +37,10 @@ def _run(pos, rdi, box, K, p, xi, rmax, alpha, beta, tol, f, z):
         assert res.returncode == 0, res.stderr
         out = np.fromfile(fout, dtype=np.float64)
     n3 = 3 * N
-    parts = np.split(out, np.cumsum([nr * n3] * 3 + [n3]))
+    parts = np.split(out, np.cumsum([nr * n3] * 3 + [n3, nr * n3]))
     return {"v_full": parts[0].reshape(nr, n3), "v_real": parts[1].reshape(nr, n3),
-            "v_recip": parts[2].reshape(nr, n3), "y1": parts[3], "y": parts[4].reshape(nr, n3)}
+            "v_recip": parts[2].reshape(nr, n3), "y1": parts[3], "y": parts[4].reshape(nr, n3),
+            "v_ewald": parts[5].reshape(nr, n3)}
 
 
 @pytest.mark.skipif(not os.access(EXE, os.X_OK), reason="adapter_parity not built (needs the reference headers)")
@@ -51,6 +53,8 @@ def test_reference_tests_through_cpp_adapters(gpu_available):
     # testspme.cc: SPME against the dense Ewald product, and against the
     # reference's own MobSpme on the same inputs
     assert rel_err(g["v_ewald"], out["v_full"]) < 1e-6
+    # MobEwaldGpu through MobBase against the reference's MobEwald (FP64)
+    assert rel_err(g["v_ewald"], out["v_ewald"]) < 1e-10
     for key in ("v_full", "v_real", "v_recip"):
         assert rel_err(g[key], out[key]) < 1e-6, key
     # testlanczos.cc: Lanczos against the dense symmetric square root, 1 and 3 RHS

@@ -312,6 +312,19 @@ int sdt_serve_submit(sdt_serve *h, int sys_id, int kind, int nrhs, const double 
 int sdt_serve_wait(sdt_serve *h, long long ticket, double timeout_ms, double *latency_ms);
 
 int sdt_serve_stats(sdt_serve *h, long long *completed, long long *rejected, double *used_bytes);
+
+/* Continuous batching: requests on monodisperse systems with grid dimension
+ * <= 256 and at most 16 RHS are served by two batch lanes.  A free lane takes
+ * the oldest waiting request together with every other waiting request of the
+ * same kind and RHS count on an idle system (up to 32) and runs them as one
+ * packed product or one lockstep block Lanczos over their systems; requests
+ * that arrive meanwhile join the next batch, and the two lanes' batches
+ * overlap on the device.  A lane's workspace (grid slots and Krylov bases for
+ * every such system) is charged to the HBM budget; a lane that does not fit
+ * stays idle.  Set STOKESDT_SERVE_BATCH=0 at create to serve every request
+ * alone.  Reports the batches run, the requests they held and the lanes in
+ * use (any pointer may be NULL). */
+int sdt_serve_batch_stats(sdt_serve *h, long long *batches, long long *batched_requests, int *lanes_active);
 const char *sdt_serve_last_error(sdt_serve *h);
 void sdt_serve_destroy(sdt_serve *h);
 

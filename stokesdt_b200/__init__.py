@@ -122,6 +122,8 @@ SIGNATURES = {
     "sdt_serve_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_double)]),
     "sdt_serve_last_error": (ctypes.c_char_p, [_vp]),
+    "sdt_serve_batch_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.POINTER(ctypes.c_longlong), _ip]),
     "sdt_serve_destroy": (None, [_vp]),
     "sdt_xyz_count": (ctypes.c_int, [ctypes.c_char_p, _ip]),
     "sdt_xyz_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, _dp, _dp, _dp, _ip,
@@ -756,7 +758,10 @@ class MobilityServer:
     def stats(self):
         c, r, u = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_double(0.0)
         lib().sdt_serve_stats(self._h, ctypes.byref(c), ctypes.byref(r), ctypes.byref(u))
-        return {"completed": c.value, "rejected": r.value, "used_bytes": u.value}
+        b, br, la = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_int(0)
+        lib().sdt_serve_batch_stats(self._h, ctypes.byref(b), ctypes.byref(br), ctypes.byref(la))
+        return {"completed": c.value, "rejected": r.value, "used_bytes": u.value, "batches": b.value,
+                "batched_requests": br.value, "batch_lanes": la.value}
 
     def close(self):
         if self._h is not None:

@@ -239,6 +239,16 @@ int sdt_serve_stats(sdt_serve *h, long long *completed, long long *rejected, dou
     return SDT_OK;
 }
 
+int sdt_serve_batch_stats(sdt_serve *h, long long *batches, long long *batched_requests, int *lanes_active)
+{
+    if (!h) return SDT_ERR_INVALID;
+    std::lock_guard<std::mutex> g(h->s.mu);
+    if (batches) *batches = h->s.batches;
+    if (batched_requests) *batched_requests = h->s.batched_requests;
+    if (lanes_active) *lanes_active = h->s.lanes_active;
+    return SDT_OK;
+}
+
 const char *sdt_serve_last_error(sdt_serve *h)
 {
     if (!h) return "";

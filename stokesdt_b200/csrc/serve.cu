@@ -10,9 +10,20 @@
 // taken by `lanes` workers (a CUDA stream, a host thread and a Lanczos
 // workspace each); a system serves one request at a time, so requests on
 // different systems overlap and requests on one system keep their order.
+//
+// Continuous batching (monodisperse systems with K <= 256, requests of at
+// most 16 RHS): two batch lanes, each with a packed product state and a
+// batched block Lanczos over all such systems (packed.h,
+// packed_lanczos.h).  A free lane takes the oldest waiting request and every
+// other waiting request of the same kind and RHS count on an idle system (up
+// to max_batch) and runs them as one packed product or one lockstep Lanczos;
+// requests that arrive meanwhile join the next batch, and the two lanes'
+// batches overlap on the device.  Other requests go to the per-request
+// workers.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "serve.h"
@@ -55,7 +66,19 @@ int serve_create(ServeState *sv, int device, size_t budget, int lanes, int max_n
     sv->budget = budget;
     sv->max_npos = max_npos;
     sv->max_nrhs = max_nrhs;
+    sv->max_iters = max_iters;
+    sv->tol = tol;
+    const char *env = std::getenv("STOKESDT_SERVE_BATCH");
+    sv->batching = !(env && env[0] == '0');
     if (cudaSetDevice(device) != cudaSuccess) return serve_error(sv, kErrCuda, "cudaSetDevice failed");
+    if (sv->batching) {
+        // the per-request workers only serve what the batch lanes cannot take
+        lanes = 1;
+        sv->blanes.resize(2);
+        for (ServeBatchLane &bl : sv->blanes)
+            if (cudaStreamCreateWithFlags(&bl.stream, cudaStreamNonBlocking) != cudaSuccess)
+                return serve_error(sv, kErrCuda, "stream creation failed");
+    }
     sv->workers.resize(lanes);
     for (int l = 0; l < lanes; l++) {
         ServeWorker &w = sv->workers[l];
@@ -78,7 +101,15 @@ int serve_create(ServeState *sv, int device, size_t budget, int lanes, int max_n
         }
     }
     for (int l = 0; l < lanes; l++) sv->workers[l].th = std::thread(serve_worker_loop, sv, l);
+    for (size_t l = 0; l < sv->blanes.size(); l++) sv->blanes[l].th = std::thread(serve_batch_loop, sv, (int)l);
     return kOk;
+}
+
+// Whether request r goes to a batch lane (caller holds the lock).
+static bool batchable(const ServeState *sv, const ServeRequest &r)
+{
+    return sv->batching && sv->systems[r.sys]->packable && r.nrhs <= std::min(sv->max_nrhs, kBlMaxK) &&
+           (sv->pk_dirty || sv->rebuilding || sv->lanes_active > 0);
 }
 
 int serve_register(ServeState *sv, int npos, const double *rdi, double box, int K, double xi, double rmax,
@@ -120,8 +151,15 @@ int serve_register(ServeState *sv, int npos, const double *rdi, double box, int 
         st = kErrCuda;
     if (st == kOk) st = spme_update(e, s->d_pos);
     if (st == kOk && cudaStreamSynchronize(e->stream) != cudaSuccess) st = kErrCuda;
+    if (st == kOk && (cudaMalloc(&s->d_in, (size_t)sv->max_nrhs * 3 * npos * sizeof(double)) != cudaSuccess ||
+                      cudaMalloc(&s->d_out, (size_t)sv->max_nrhs * 3 * npos * sizeof(double)) != cudaSuccess)) {
+        cudaGetLastError();
+        st = kErrAlloc;
+    }
     if (st != kOk) {
         const std::string msg = e->last_error;
+        cudaFree(s->d_in);
+        cudaFree(s->d_out);
         cudaFree(s->d_pos);
         spme_free(e);
         delete s;
@@ -134,9 +172,87 @@ int serve_register(ServeState *sv, int npos, const double *rdi, double box, int 
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     e->own_stream = false;
     e->stream = nullptr;
+    s->packable = sv->batching && e->mono && e->K <= 256 && e->tma_enabled && e->tma_tabs && e->zfused;
     std::lock_guard<std::mutex> g(sv->mu);
     sv->systems.push_back(s);
     *sys_id = (int)sv->systems.size() - 1;
+    // the batch lanes rebuild their packed state before their next batch
+    if (s->packable) sv->pk_dirty = true;
+    return kOk;
+}
+
+// Rebuilds every batch lane's packed product state and batched Lanczos
+// workspace over the packable systems (no lane busy; lock not held).  Lanes
+// whose workspace does not fit the HBM budget stay idle.
+static int rebuild_lanes(ServeState *sv)
+{
+    cudaSetDevice(sv->device);
+    std::vector<int> ids;
+    std::vector<SpmeEngine *> eng;
+    std::vector<int> npos;
+    {
+        std::lock_guard<std::mutex> g(sv->mu);
+        for (size_t i = 0; i < sv->systems.size(); i++)
+            if (sv->systems[i]->packable) {
+                sv->systems[i]->pk = (int)ids.size();
+                ids.push_back((int)i);
+                eng.push_back(&sv->systems[i]->eng);
+                npos.push_back(sv->systems[i]->eng.npos);
+            }
+        sv->pk_sys = ids;
+        sv->used -= sv->lane_bytes;
+        sv->lane_bytes = 0;
+    }
+    int active = 0;
+    const int rhs = std::min(sv->max_nrhs, kBlMaxK);
+    // estimated bytes of one lane: class grids, FP32 work, Krylov bases
+    size_t per_lane = 0;
+    for (SpmeEngine *e : eng) {
+        const size_t n3 = 3 * (size_t)e->npos, ld = (n3 + 31) / 32 * 32;
+        per_lane += (size_t)rhs * 3 * e->K * e->K * e->XS * sizeof(float2) + (size_t)e->K * e->K * e->XS * 4 +
+                    (size_t)e->npos * rhs * 13 * 4 + (size_t)(sv->max_iters + 1) * rhs * ld * 8;
+    }
+    int st = kOk;
+    for (size_t l = 0; l < sv->blanes.size(); l++) {
+        ServeBatchLane &bl = sv->blanes[l];
+        if (bl.bl) {
+            bl_free(bl.bl);
+            delete bl.bl;
+            bl.bl = nullptr;
+        }
+        if (bl.pk) {
+            packed_free(bl.pk);
+            delete bl.pk;
+            bl.pk = nullptr;
+        }
+        if (eng.empty()) continue;
+        {
+            std::lock_guard<std::mutex> g(sv->mu);
+            if (sv->used + per_lane > sv->budget) continue;
+            sv->used += per_lane;
+            sv->lane_bytes += per_lane;
+        }
+        bl.pk = new PackedBatch;
+        st = packed_create(bl.pk, eng, rhs, sv->device, bl.stream);
+        if (st == kOk) st = packed_refresh(bl.pk);
+        if (st != kOk) {
+            std::lock_guard<std::mutex> g(sv->mu);
+            sv->lanes_active = 0;
+            sv->last_error = "batch lane set-up: " + bl.pk->last_error;
+            return st;
+        }
+        bl.bl = new BLState;
+        st = bl_create(bl.bl, npos, sv->max_iters, rhs, sv->tol, sv->device, bl.stream);
+        if (st != kOk) {
+            std::lock_guard<std::mutex> g(sv->mu);
+            sv->lanes_active = 0;
+            sv->last_error = "batch lane Lanczos set-up: " + bl.bl->last_error;
+            return st;
+        }
+        active++;
+    }
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->lanes_active = active;
     return kOk;
 }
 
@@ -164,11 +280,12 @@ int serve_submit(ServeState *sv, int sys_id, int kind, int nrhs, const double *i
     return kOk;
 }
 
-// Next request whose system is idle, in arrival order (locked by the caller).
+// Next request for the per-request workers whose system is idle, in arrival
+// order (locked by the caller).
 static bool take_request(ServeState *sv, ServeRequest &r)
 {
     for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
-        if (!sv->systems[it->sys]->busy) {
+        if (!sv->systems[it->sys]->busy && !batchable(sv, *it)) {
             r = *it;
             sv->queue.erase(it);
             sv->systems[r.sys]->busy = true;
@@ -224,6 +341,137 @@ void serve_worker_loop(ServeState *sv, int lane)
     }
 }
 
+// The oldest batchable request on an idle system and every later one of the
+// same kind and RHS count on another idle system, up to max_batch (locked by
+// the caller); their systems are marked busy.
+static void take_batch(ServeState *sv, std::vector<ServeRequest> &batch)
+{
+    batch.clear();
+    int kind = -1, nrhs = -1;
+    for (auto it = sv->queue.begin(); it != sv->queue.end() && (int)batch.size() < sv->max_batch;) {
+        ServeSystem *s = sv->systems[it->sys];
+        if (!s->busy && batchable(sv, *it) && s->pk >= 0 &&
+            (kind < 0 || (it->kind == kind && it->nrhs == nrhs))) {
+            kind = it->kind;
+            nrhs = it->nrhs;
+            s->busy = true;
+            batch.push_back(*it);
+            it = sv->queue.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+static bool has_batch_work(ServeState *sv)
+{
+    for (const ServeRequest &r : sv->queue)
+        if (!sv->systems[r.sys]->busy && batchable(sv, r)) return true;
+    return false;
+}
+
+// One batch on lane `lane`: copy the inputs in, one packed product or one
+// lockstep block Lanczos over the batch's systems, copy the outputs out.
+static int run_batch(ServeState *sv, ServeBatchLane &bl, const std::vector<ServeRequest> &batch)
+{
+    const int nb = (int)batch.size(), kind = batch[0].kind, k = batch[0].nrhs;
+    std::vector<int> act(nb), ld(nb), it(nb, 0);
+    std::vector<const double *> f(nb);
+    std::vector<double *> v(nb);
+    for (int j = 0; j < nb; j++) {
+        ServeSystem *s = sv->systems[batch[j].sys];
+        const size_t n3 = 3 * (size_t)s->eng.npos;
+        if (cudaMemcpyAsync(s->d_in, batch[j].in, (size_t)k * n3 * sizeof(double), cudaMemcpyHostToDevice,
+                            bl.stream) != cudaSuccess)
+            return kErrCuda;
+        act[j] = s->pk;
+        ld[j] = (int)n3;
+        f[j] = s->d_in;
+        v[j] = s->d_out;
+    }
+    int st;
+    if (kind == 0) {
+        st = packed_mulvec(bl.pk, nb, act.data(), k, 1.0, f.data(), ld.data(), 0.0, v.data(), ld.data());
+        if (st != kOk) serve_error(sv, st, "batched product: " + bl.pk->last_error);
+    } else {
+        st = bl_compute(bl.bl, bl.pk, act, k, f.data(), ld.data(), v.data(), ld.data(), it.data());
+        if (st == kErrNotConverged) st = kOk;  // logged by the reference, result kept
+        if (st != kOk) serve_error(sv, st, "batched Lanczos: " + bl.bl->last_error);
+    }
+    if (st != kOk) return st;
+    for (int j = 0; j < nb; j++) {
+        ServeSystem *s = sv->systems[batch[j].sys];
+        const size_t n3 = 3 * (size_t)s->eng.npos;
+        if (cudaMemcpyAsync(batch[j].out, s->d_out, (size_t)k * n3 * sizeof(double), cudaMemcpyDeviceToHost,
+                            bl.stream) != cudaSuccess)
+            return kErrCuda;
+    }
+    if (cudaStreamSynchronize(bl.stream) != cudaSuccess) return kErrCuda;
+    st = packed_check_error(bl.pk);
+    if (st != kOk) serve_error(sv, st, bl.pk->last_error);
+    return st;
+}
+
+void serve_batch_loop(ServeState *sv, int lane)
+{
+    ServeBatchLane &bl = sv->blanes[lane];
+    cudaSetDevice(sv->device);
+    std::vector<ServeRequest> batch;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            sv->cv.wait(lk, [&] {
+                return sv->stopping || (!sv->rebuilding && (sv->pk_dirty || (bl.pk && has_batch_work(sv))));
+            });
+            if (sv->stopping) return;
+            if (sv->pk_dirty) {
+                bool others_busy = false;
+                for (const ServeBatchLane &o : sv->blanes) others_busy = others_busy || o.busy;
+                if (others_busy) {
+                    sv->cv.wait(lk, [&] {
+                        bool b = false;
+                        for (const ServeBatchLane &o : sv->blanes) b = b || o.busy;
+                        return sv->stopping || !b;
+                    });
+                    continue;
+                }
+                // a registration during the rebuild sets pk_dirty again
+                sv->rebuilding = true;
+                sv->pk_dirty = false;
+                lk.unlock();
+                const int st = rebuild_lanes(sv);
+                lk.lock();
+                sv->rebuilding = false;
+                if (st != kOk || sv->lanes_active == 0) {
+                    // no lane could be set up: the workers take everything
+                    for (ServeSystem *s : sv->systems) s->packable = false;
+                }
+                sv->cv.notify_all();
+                continue;
+            }
+            if (!bl.pk) continue;  // this lane's workspace did not fit the budget
+            take_batch(sv, batch);
+            if (batch.empty()) continue;
+            bl.busy = true;
+        }
+        const int st = run_batch(sv, bl, batch);
+        const double t_done = now_ms();
+        {
+            std::lock_guard<std::mutex> g(sv->mu);
+            bl.busy = false;
+            sv->batches++;
+            sv->batched_requests += (long long)batch.size();
+            for (const ServeRequest &r : batch) {
+                sv->systems[r.sys]->busy = false;
+                sv->status[r.id] = st;
+                sv->latency_ms[r.id] = t_done - r.t_submit;
+                sv->completed++;
+            }
+        }
+        sv->cv.notify_all();
+    }
+}
+
 int serve_wait(ServeState *sv, long long ticket, double timeout_ms, double *latency_ms)
 {
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -249,7 +497,21 @@ void serve_free(ServeState *sv)
     sv->cv.notify_all();
     for (ServeWorker &w : sv->workers)
         if (w.th.joinable()) w.th.join();
+    for (ServeBatchLane &bl : sv->blanes)
+        if (bl.th.joinable()) bl.th.join();
     cudaSetDevice(sv->device);
+    for (ServeBatchLane &bl : sv->blanes) {
+        if (bl.bl) {
+            bl_free(bl.bl);
+            delete bl.bl;
+        }
+        if (bl.pk) {
+            packed_free(bl.pk);
+            delete bl.pk;
+        }
+        if (bl.stream) cudaStreamDestroy(bl.stream);
+    }
+    sv->blanes.clear();
     for (ServeWorker &w : sv->workers) {
         if (w.stream) cudaStreamSynchronize(w.stream);
         if (w.lz) {
@@ -267,6 +529,8 @@ void serve_free(ServeState *sv)
         s->eng.stream = nullptr;
         spme_free(&s->eng);
         cudaFree(s->d_pos);
+        cudaFree(s->d_in);
+        cudaFree(s->d_out);
         delete s;
     }
     sv->systems.clear();

@@ -12,6 +12,8 @@
 
 #include "engine.h"
 #include "lanczos.h"
+#include "packed.h"
+#include "packed_lanczos.h"
 
 namespace sdt {
 
@@ -20,8 +22,11 @@ constexpr int kPending = 1;  // request status while queued or running
 struct ServeSystem {
     SpmeEngine eng;
     double *d_pos = nullptr;
+    double *d_in = nullptr, *d_out = nullptr;  // request vectors (max_nrhs x 3 npos each)
     size_t bytes = 0;   // admitted device-memory estimate
-    bool busy = false;  // a worker is running a request on it
+    bool busy = false;  // a worker or a batch lane is running a request on it
+    bool packable = false;  // monodisperse with K <= 256: served by the batch lanes
+    int pk = -1;            // index in the batch lanes' packed set (-1 until built)
 };
 
 struct ServeRequest {
@@ -41,6 +46,17 @@ struct ServeWorker {
     std::thread th;
 };
 
+// A batch lane: runs batches of requests (one kind, one RHS count, distinct
+// systems) as one packed product or one lockstep block Lanczos over their
+// systems, on its own stream with its own packed state.
+struct ServeBatchLane {
+    cudaStream_t stream = nullptr;
+    PackedBatch *pk = nullptr;
+    BLState *bl = nullptr;
+    std::thread th;
+    bool busy = false;
+};
+
 struct ServeState {
     int device = 0;
     size_t budget = 0, used = 0;
@@ -49,6 +65,16 @@ struct ServeState {
     bool stopping = false;
     std::vector<ServeSystem *> systems;
     std::vector<ServeWorker> workers;
+    // continuous batching (monodisperse systems with K <= 256)
+    bool batching = true;            // cleared by STOKESDT_SERVE_BATCH=0
+    int max_iters = 0, max_batch = 32;
+    double tol = 0.0;
+    std::vector<ServeBatchLane> blanes;
+    std::vector<int> pk_sys;         // packed index -> system id
+    bool pk_dirty = false, rebuilding = false;
+    size_t lane_bytes = 0;           // device memory of the batch lanes' workspaces
+    int lanes_active = 0;            // batch lanes whose workspace fits the budget
+    long long batches = 0, batched_requests = 0;
     std::deque<ServeRequest> queue;
     std::map<long long, int> status;
     std::map<long long, double> latency_ms;
@@ -65,6 +91,7 @@ int serve_register(ServeState *sv, int npos, const double *rdi, double box, int 
 int serve_submit(ServeState *sv, int sys_id, int kind, int nrhs, const double *in, double *out, long long *ticket);
 int serve_wait(ServeState *sv, long long ticket, double timeout_ms, double *latency_ms);
 void serve_worker_loop(ServeState *sv, int lane);
+void serve_batch_loop(ServeState *sv, int lane);
 void serve_free(ServeState *sv);
 
 }  // namespace sdt

@@ -79,3 +79,50 @@ def test_admission_by_hbm_budget(gpu_available):
     with pytest.raises(sdt.StokesError):
         srv.submit(sid, 0, 8, np.ones((8, 3 * s0["npos"])), np.zeros((8, 3 * s0["npos"])))  # > max_nrhs
     srv.close()
+
+
+def test_mix_formed_while_a_batch_is_in_flight(gpu_available):
+    """Continuous batching: a Brownian batch (k = 16 on every system) is in
+    flight when mobility applies on the same systems arrive; they wait for
+    their systems and run together as later batches.  Every result equals the
+    same request served alone on a fresh server (1e-6 for M.f, 1e-5 for
+    sqrt(M) z), and the batches held more than one request each on average."""
+    import stokesdt_b200 as sdt
+    sy = _systems()
+
+    def server():
+        srv = sdt.MobilityServer(hbm_budget_bytes=20e9, lanes=2, max_npos=2000, max_iters=100, max_nrhs=16,
+                                 tol=1e-6)
+        ids = [srv.register(s["npos"], np.ones(s["npos"]), s["box"], s["K"], s["xi"], s["rmax"], 6, s["pos"])
+               for s in sy]
+        return srv, ids
+
+    rng = np.random.default_rng(11)
+    inputs = []
+    for i, s in enumerate(sy):
+        n3 = 3 * s["npos"]
+        inputs.append((i, 1, 16, rng.standard_normal((16, n3))))
+    for i, s in enumerate(sy):
+        n3 = 3 * s["npos"]
+        inputs.append((i, 0, 4, rng.standard_normal((4, n3))))
+        inputs.append((i, 0, 1, rng.standard_normal((1, n3))))
+    srv, ids = server()
+    outs, tickets = [], []
+    for (i, kind, k, x) in inputs:
+        out = np.zeros_like(x)
+        outs.append(out)
+        tickets.append(srv.submit(ids[i], kind, k, x, out))
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    assert st["completed"] == len(inputs)
+    assert st["batch_lanes"] >= 1 and st["batches"] >= 1
+    assert st["batched_requests"] == len(inputs) and st["batched_requests"] > st["batches"]
+    srv.close()
+    # each request alone
+    for (i, kind, k, x), out in zip(inputs, outs):
+        srv, ids = server()
+        ref = np.zeros_like(x)
+        srv.wait(srv.submit(ids[i], kind, k, x, ref))
+        srv.close()
+        assert rel_err(ref, out) < (1e-6 if kind == 0 else 1e-5), (i, kind, k)

@@ -956,41 +956,62 @@ def serve_requests(nsys: int, nreq: int, rate: float, seed: int):
 
 
 def run_b200_serve(args):
-    """Config 5: a served request stream on one GPU (sdt_serve_*): systems
-    with N log-uniform in [1e3, 1e5] and phi uniform in [0.05, 0.3] are
-    registered once (device-resident, admitted by HBM budget); requests
-    arrive as a Poisson stream at swept rates.  Reported: throughput and
-    p50/p99 latency per rate, and the plain per-request path (engine built,
-    updated, used and released per request, one at a time) on the same
-    requests."""
-    import threading
+    """Config 5: a served request stream (sdt_serve_*): systems with N
+    log-uniform in [1e3, 1e5] and phi uniform in [0.05, 0.3] are registered
+    once (device-resident, admitted by HBM budget); requests arrive as a
+    Poisson stream at swept rates, plus one burst (every request at t = 0)
+    that measures capacity.  Under torchrun the systems are split over the
+    ranks by cost (largest first onto the least-loaded rank) and each rank
+    serves the requests on its own systems: no data is exchanged, NCCL carries
+    only the barrier and the max over ranks.  A rate's span runs from the
+    common start to the slowest rank's last completion; throughput = all
+    ranks' requests / that span.  Also reported: p50/p99 latency over all
+    requests, the continuous-batching counts, and (rank 0) the plain
+    per-request path (engine built, updated, used and released per request,
+    one at a time) on the same requests."""
     import torch
     import stokesdt_b200 as sdt
     from stokesdt_b200 import workloads as wl
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    rank = int(os.environ.get("RANK", "0"))
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     rng = np.random.default_rng(41)
-    nsys = 12
+    nsys = 12 * world
     npos = np.exp(rng.uniform(np.log(1e3), np.log(1e5), nsys)).astype(int)
     phis = rng.uniform(0.05, 0.3, nsys)
     systems = []
     for s in range(nsys):
         K, xi, rmax = wl.autotune_system(int(npos[s]), float(phis[s]), kmax=256)
         L = wl.box_for(int(npos[s]), float(phis[s]))
-        systems.append(dict(npos=int(npos[s]), box=L, K=K, xi=xi, rmax=rmax,
-                            pos=wl.rsa_positions(int(npos[s]), L, 4100 + s).reshape(-1)))
-    srv = sdt.MobilityServer(device=local, hbm_budget_bytes=120e9, lanes=4, max_npos=int(npos.max()),
-                             max_iters=100, max_nrhs=16, tol=1e-6)
-    ids = [srv.register(s["npos"], np.ones(s["npos"]), s["box"], s["K"], s["xi"], s["rmax"], 6, s["pos"])
-           for s in systems]
-    inputs = [np.random.default_rng(s).standard_normal((16, 3 * systems[s]["npos"])) for s in range(nsys)]
+        systems.append(dict(npos=int(npos[s]), box=L, K=K, xi=xi, rmax=rmax, seed=4100 + s))
+    mine = wl.shard_systems(systems, world, rank)
+    srv = sdt.MobilityServer(device=local, hbm_budget_bytes=120e9, lanes=4,
+                             max_npos=max(systems[s]["npos"] for s in mine), max_iters=100, max_nrhs=16, tol=1e-6)
+    ids, pos, inputs = {}, {}, {}
+    for s in mine:
+        sd = systems[s]
+        pos[s] = wl.rsa_positions(sd["npos"], sd["box"], sd["seed"]).reshape(-1)
+        ids[s] = srv.register(sd["npos"], np.ones(sd["npos"]), sd["box"], sd["K"], sd["xi"], sd["rmax"], 6, pos[s])
+        inputs[s] = np.random.default_rng(s).standard_normal((16, 3 * sd["npos"]))
 
     def serve(reqs):
+        """This rank's share of `reqs`, submitted at their arrival times from
+        the common start; returns (latencies, seconds to the last completion)."""
         outs, tickets = [], []
+        if dist is not None:
+            dist.barrier()
         t0 = time.perf_counter()
         for (ta, s, kind, k) in reqs:
+            if s not in ids:
+                continue
             dt = ta - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
@@ -999,59 +1020,93 @@ def run_b200_serve(args):
             outs.append(out)
             tickets.append(srv.submit(ids[s], kind, k, x, out))
         lat = [srv.wait(t) for t in tickets]
-        span = time.perf_counter() - t0
-        return lat, span
+        return lat, time.perf_counter() - t0
+
+    def gather(lat):
+        if dist is None:
+            return list(lat)
+        parts = [None] * world
+        dist.all_gather_object(parts, list(lat))
+        return [v for p in parts for v in p]
 
     # warm-up: every system once with each kind
-    serve([(0.0, s, kind, 4) for s in range(nsys) for kind in (0, 1)])
+    nwarm = max(1, args.warmup // 3)
+    for _ in range(nwarm):
+        serve([(0.0, s, kind, 4) for s in range(nsys) for kind in (0, 1)])
     launches0 = sdt.kernel_launches()
+    st0 = srv.stats()
     sampler = ClockSampler(local)
     sampler.start()
     per_rate = []
-    nreq = max(20, 10 * args.steps)
-    for rate in (5.0, 20.0, 80.0):
-        reqs = serve_requests(nsys, nreq, rate, seed=int(rate))
+    nreq = max(20, 10 * args.steps) * world
+    for rate in (5.0 * world, 20.0 * world, 80.0 * world, None):
+        if rate is None:
+            reqs = [(0.0, s, kind, k) for (_, s, kind, k) in serve_requests(nsys, nreq, 1.0, seed=99)]
+        else:
+            reqs = serve_requests(nsys, nreq, rate, seed=int(rate))
+        st_a = srv.stats()
         lat, span = serve(reqs)
-        per_rate.append({"offered_per_s": rate, "requests": len(reqs), "throughput_per_s": round(len(reqs) / span, 3),
+        st_b = srv.stats()
+        span = max_over_ranks(dist, span, dev)
+        lat = gather(lat)
+        nb = st_b["batches"] - st_a["batches"]
+        nbr = st_b["batched_requests"] - st_a["batched_requests"]
+        per_rate.append({"offered_per_s": rate if rate is not None else "burst", "requests": len(reqs),
+                         "throughput_per_s": round(len(reqs) / span, 3),
                          "p50_ms": round(float(np.percentile(lat, 50)), 3),
-                         "p99_ms": round(float(np.percentile(lat, 99)), 3)})
-        log(f"rate {rate}: {per_rate[-1]}")
+                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                         "batches_rank0": nb, "requests_per_batch_rank0": round(nbr / nb, 3) if nb else None})
+        if rank == 0:
+            log(f"rate {rate}: {per_rate[-1]}")
     clocks = sampler.stop()
     launches = sdt.kernel_launches() - launches0
+    st1 = srv.stats()
     srv.close()
 
-    # plain per-request path on the first requests of the lowest rate
+    # plain per-request path (rank 0, its own systems) on the first requests of the lowest rate
     plain_lat = []
-    for (_, s, kind, k) in serve_requests(nsys, min(24, nreq), 5.0, seed=5)[:24]:
-        sd = systems[s]
-        t0 = time.perf_counter()
-        m = sdt.MobSpme(sd["npos"], np.ones(sd["npos"]), sd["box"], sd["xi"], sd["rmax"], sd["K"], 6, device=local)
-        assert m.Init()
-        m.Update(sd["pos"])
-        n3 = 3 * sd["npos"]
-        x = np.ascontiguousarray(inputs[s][:k])
-        out = np.zeros_like(x)
-        if kind == 0:
-            m.MulVector(k, 1.0, n3, x, 0.0, n3, out)
-        else:
-            lz = sdt.BrwnLanczos(n3, 100, 16, 1e-6, device=local, reorth=True)
-            assert lz.Init()
-            lz.Compute(m, k, n3, x, n3, out)
-            del lz
-        del m
-        plain_lat.append(1e3 * (time.perf_counter() - t0))
+    if rank == 0:
+        for (_, s, kind, k) in serve_requests(nsys, 4 * nreq, 5.0, seed=5):
+            if s not in ids:
+                continue
+            if len(plain_lat) == 24:
+                break
+            sd = systems[s]
+            t0 = time.perf_counter()
+            m = sdt.MobSpme(sd["npos"], np.ones(sd["npos"]), sd["box"], sd["xi"], sd["rmax"], sd["K"], 6,
+                            device=local)
+            assert m.Init()
+            m.Update(pos[s])
+            n3 = 3 * sd["npos"]
+            x = np.ascontiguousarray(inputs[s][:k])
+            out = np.zeros_like(x)
+            if kind == 0:
+                m.MulVector(k, 1.0, n3, x, 0.0, n3, out)
+            else:
+                lz = sdt.BrwnLanczos(n3, 100, 16, 1e-6, device=local, reorth=True)
+                assert lz.Init()
+                lz.Compute(m, k, n3, x, n3, out)
+                del lz
+            del m
+            plain_lat.append(1e3 * (time.perf_counter() - t0))
     if rank == 0:
         best = max(per_rate, key=lambda r: r["throughput_per_s"])
         out = {
             "metric": "served requests/s (config 5) and p50/p99 latency", "value": best["throughput_per_s"],
-            "unit": "requests/s", "n_gpus": 1, "steps": nreq, "warmup": 2 * nsys,
+            "unit": "requests/s", "n_gpus": world, "steps": nreq, "warmup": 2 * nsys * nwarm,
             "ms_per_step": round(1e3 / best["throughput_per_s"], 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": "Poisson request stream: mobility apply or Brownian step, k in {1,4,16}, "
-                                   "12 systems N log-uniform [1e3, 1e5], phi U[0.05, 0.3], p=6, tol 1e-6",
-                       "lanes": 4, "hbm_budget_gb": 120, "systems": [(s["npos"], s["K"]) for s in systems],
+                                   f"{nsys} systems (12 per GPU) N log-uniform [1e3, 1e5], phi U[0.05, 0.3], "
+                                   "p=6, tol 1e-6; offered rates 5/20/80 per s per GPU and a burst",
+                       "lanes": 4, "hbm_budget_gb": 120,
+                       "systems_rank0": [(systems[s]["npos"], systems[s]["K"]) for s in mine],
+                       "parallelism": f"systems sharded over {world} GPU(s) by cost, no data exchange",
                        "l2": "no flush: systems' grids exceed the 126 MB L2"},
             "per_rate": per_rate,
+            "batching_rank0": {"batch_lanes": st1["batch_lanes"], "batches": st1["batches"] - st0["batches"],
+                               "batched_requests": st1["batched_requests"] - st0["batched_requests"],
+                               "completed": st1["completed"] - st0["completed"]},
             "plain_per_request_path": {"requests": len(plain_lat),
                                        "p50_ms": round(float(np.percentile(plain_lat, 50)), 3),
                                        "p99_ms": round(float(np.percentile(plain_lat, 99)), 3),
@@ -1061,6 +1116,9 @@ def run_b200_serve(args):
             "gpu_launches": int(launches), "clocks": clocks,
         }
         print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():

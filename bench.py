@@ -955,6 +955,37 @@ def serve_requests(nsys: int, nreq: int, rate: float, seed: int):
             for i in range(nreq)]
 
 
+def serve_systems(world: int):
+    """Config 5 systems, 12 per rank: N log-uniform in [1e3, 1e5], phi
+    uniform in [0.05, 0.3], grid / xi / rmax from the autotuner (K <= 256)."""
+    from stokesdt_b200 import workloads as wl
+    rng = np.random.default_rng(41)
+    nsys = 12 * world
+    npos = np.exp(rng.uniform(np.log(1e3), np.log(1e5), nsys)).astype(int)
+    phis = rng.uniform(0.05, 0.3, nsys)
+    systems = []
+    for s in range(nsys):
+        K, xi, rmax = wl.autotune_system(int(npos[s]), float(phis[s]), kmax=256)
+        L = wl.box_for(int(npos[s]), float(phis[s]))
+        systems.append(dict(npos=int(npos[s]), box=L, K=K, xi=xi, rmax=rmax, seed=4100 + s))
+    return systems
+
+
+def rank_share(reqs, mine):
+    """The requests of `reqs` whose system this rank serves."""
+    own = set(mine)
+    return [r for r in reqs if r[1] in own]
+
+
+def gather_all(dist, vals, world: int):
+    """Every rank's list of values, concatenated in rank order."""
+    if dist is None:
+        return list(vals)
+    parts = [None] * world
+    dist.all_gather_object(parts, list(vals))
+    return [v for p in parts for v in p]
+
+
 def run_b200_serve(args):
     """Config 5: a served request stream (sdt_serve_*): systems with N
     log-uniform in [1e3, 1e5] and phi uniform in [0.05, 0.3] are registered
@@ -983,15 +1014,8 @@ def run_b200_serve(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-    rng = np.random.default_rng(41)
-    nsys = 12 * world
-    npos = np.exp(rng.uniform(np.log(1e3), np.log(1e5), nsys)).astype(int)
-    phis = rng.uniform(0.05, 0.3, nsys)
-    systems = []
-    for s in range(nsys):
-        K, xi, rmax = wl.autotune_system(int(npos[s]), float(phis[s]), kmax=256)
-        L = wl.box_for(int(npos[s]), float(phis[s]))
-        systems.append(dict(npos=int(npos[s]), box=L, K=K, xi=xi, rmax=rmax, seed=4100 + s))
+    systems = serve_systems(world)
+    nsys = len(systems)
     mine = wl.shard_systems(systems, world, rank)
     srv = sdt.MobilityServer(device=local, hbm_budget_bytes=120e9, lanes=4,
                              max_npos=max(systems[s]["npos"] for s in mine), max_iters=100, max_nrhs=16, tol=1e-6)
@@ -1009,9 +1033,7 @@ def run_b200_serve(args):
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        for (ta, s, kind, k) in reqs:
-            if s not in ids:
-                continue
+        for (ta, s, kind, k) in rank_share(reqs, mine):
             dt = ta - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
@@ -1021,13 +1043,6 @@ def run_b200_serve(args):
             tickets.append(srv.submit(ids[s], kind, k, x, out))
         lat = [srv.wait(t) for t in tickets]
         return lat, time.perf_counter() - t0
-
-    def gather(lat):
-        if dist is None:
-            return list(lat)
-        parts = [None] * world
-        dist.all_gather_object(parts, list(lat))
-        return [v for p in parts for v in p]
 
     # warm-up: every system once with each kind
     nwarm = max(1, args.warmup // 3)
@@ -1048,7 +1063,7 @@ def run_b200_serve(args):
         lat, span = serve(reqs)
         st_b = srv.stats()
         span = max_over_ranks(dist, span, dev)
-        lat = gather(lat)
+        lat = gather_all(dist, lat, world)
         nb = st_b["batches"] - st_a["batches"]
         nbr = st_b["batched_requests"] - st_a["batched_requests"]
         per_rate.append({"offered_per_s": rate if rate is not None else "burst", "requests": len(reqs),

@@ -14,12 +14,15 @@
 // Continuous batching (monodisperse systems with K <= 256, requests of at
 // most 16 RHS): two batch lanes, each with a packed product state and a
 // batched block Lanczos over all such systems (packed.h,
-// packed_lanczos.h).  A free lane takes the oldest waiting request and every
-// other waiting request of the same kind and RHS count on an idle system (up
-// to max_batch) and runs them as one packed product or one lockstep Lanczos;
-// requests that arrive meanwhile join the next batch, and the two lanes'
-// batches overlap on the device.  Other requests go to the per-request
-// workers.
+// packed_lanczos.h).  A free lane takes the oldest waiting request that has
+// a partner -- another waiting request of the same kind and RHS count on
+// another idle system -- with every such partner (up to max_batch), and runs
+// them as one packed product or one lockstep Lanczos; requests that arrive
+// meanwhile join the next batch, and the two lanes' batches overlap on the
+// device.  A request without a partner goes to a per-request worker (a lone
+// request runs faster there), or to a free batch lane when every worker is
+// busy.  STOKESDT_SERVE_BATCH=all sends every batchable request to the batch
+// lanes (one worker is kept for the rest); =0 turns batching off.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -70,10 +73,10 @@ int serve_create(ServeState *sv, int device, size_t budget, int lanes, int max_n
     sv->tol = tol;
     const char *env = std::getenv("STOKESDT_SERVE_BATCH");
     sv->batching = !(env && env[0] == '0');
+    sv->batch_all = sv->batching && env && std::string(env) == "all";
     if (cudaSetDevice(device) != cudaSuccess) return serve_error(sv, kErrCuda, "cudaSetDevice failed");
     if (sv->batching) {
-        // the per-request workers only serve what the batch lanes cannot take
-        lanes = 1;
+        if (sv->batch_all) lanes = 1;  // the worker only serves what the batch lanes cannot take
         sv->blanes.resize(2);
         for (ServeBatchLane &bl : sv->blanes)
             if (cudaStreamCreateWithFlags(&bl.stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -105,11 +108,22 @@ int serve_create(ServeState *sv, int device, size_t budget, int lanes, int max_n
     return kOk;
 }
 
-// Whether request r goes to a batch lane (caller holds the lock).
+// Whether request r may go to a batch lane (caller holds the lock).
 static bool batchable(const ServeState *sv, const ServeRequest &r)
 {
     return sv->batching && sv->systems[r.sys]->packable && r.nrhs <= std::min(sv->max_nrhs, kBlMaxK) &&
            (sv->pk_dirty || sv->rebuilding || sv->lanes_active > 0);
+}
+
+// Whether another waiting request could share a batch with r: same kind and
+// RHS count, batchable, on another idle system (caller holds the lock).
+static bool has_partner(const ServeState *sv, const ServeRequest &r)
+{
+    for (const ServeRequest &o : sv->queue)
+        if (o.id != r.id && o.sys != r.sys && o.kind == r.kind && o.nrhs == r.nrhs &&
+            !sv->systems[o.sys]->busy && batchable(sv, o))
+            return true;
+    return false;
 }
 
 int serve_register(ServeState *sv, int npos, const double *rdi, double box, int K, double xi, double rmax,
@@ -150,6 +164,10 @@ int serve_register(ServeState *sv, int npos, const double *rdi, double box, int 
             cudaSuccess)
         st = kErrCuda;
     if (st == kOk) st = spme_update(e, s->d_pos);
+    // the grid work space for max_nrhs vectors now (the admission estimate
+    // counts it): a first request must not allocate, which would also stall
+    // the other lanes' streams
+    if (st == kOk) st = spme_reserve(e, std::min(sv->max_nrhs, e->rhs_chunk_max));
     if (st == kOk && cudaStreamSynchronize(e->stream) != cudaSuccess) st = kErrCuda;
     if (st == kOk && (cudaMalloc(&s->d_in, (size_t)sv->max_nrhs * 3 * npos * sizeof(double)) != cudaSuccess ||
                       cudaMalloc(&s->d_out, (size_t)sv->max_nrhs * 3 * npos * sizeof(double)) != cudaSuccess)) {
@@ -281,14 +299,21 @@ int serve_submit(ServeState *sv, int sys_id, int kind, int nrhs, const double *i
 }
 
 // Next request for the per-request workers whose system is idle, in arrival
-// order (locked by the caller).
+// order: one the batch lanes cannot take, a batchable one without a
+// partner, or any while no batch lane is free (locked by the caller).
 static bool take_request(ServeState *sv, ServeRequest &r)
 {
+    bool lane_free = false;  // (the lanes' states are rebuilt without the lock)
+    if (!sv->rebuilding)
+        for (const ServeBatchLane &bl : sv->blanes) lane_free = lane_free || (bl.pk && !bl.busy);
     for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
-        if (!sv->systems[it->sys]->busy && !batchable(sv, *it)) {
+        if (!sv->systems[it->sys]->busy &&
+            (!batchable(sv, *it) ||
+             (!sv->batch_all && (!lane_free || sv->rebuilding || !has_partner(sv, *it))))) {
             r = *it;
             sv->queue.erase(it);
             sv->systems[r.sys]->busy = true;
+            sv->workers_busy++;
             return true;
         }
     }
@@ -306,6 +331,7 @@ void serve_worker_loop(ServeState *sv, int lane)
             sv->cv.wait(lk, [&] { return sv->stopping || take_request(sv, r); });
             if (sv->stopping && r.id < 0) return;
         }
+        sv->cv.notify_all();  // a batch lane may take lone requests now that this worker is busy
         ServeSystem *s = sv->systems[r.sys];
         SpmeEngine *e = &s->eng;
         const int n3 = 3 * e->npos;
@@ -332,6 +358,7 @@ void serve_worker_loop(ServeState *sv, int lane)
         {
             std::lock_guard<std::mutex> g(sv->mu);
             s->busy = false;
+            sv->workers_busy--;
             sv->status[r.id] = st == kOk ? kOk : st;
             sv->latency_ms[r.id] = t_done - r.t_submit;
             sv->completed++;
@@ -341,19 +368,35 @@ void serve_worker_loop(ServeState *sv, int lane)
     }
 }
 
-// The oldest batchable request on an idle system and every later one of the
-// same kind and RHS count on another idle system, up to max_batch (locked by
-// the caller); their systems are marked busy.
+// The request a batch lane starts its next batch with: the oldest batchable
+// request on an idle system that has a partner, or, when every worker is
+// busy, the oldest batchable request on an idle system (locked by the
+// caller); queue end if none.
+static std::deque<ServeRequest>::iterator batch_head(ServeState *sv)
+{
+    const bool workers_full = sv->batch_all || sv->workers_busy >= (int)sv->workers.size();
+    auto lone = sv->queue.end();
+    for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
+        const ServeSystem *s = sv->systems[it->sys];
+        if (s->busy || s->pk < 0 || !batchable(sv, *it)) continue;
+        if (has_partner(sv, *it)) return it;
+        if (workers_full && lone == sv->queue.end()) lone = it;
+    }
+    return lone;
+}
+
+// The batch head and every later request of its kind and RHS count on
+// another idle system, up to max_batch (locked by the caller); their systems
+// are marked busy.
 static void take_batch(ServeState *sv, std::vector<ServeRequest> &batch)
 {
     batch.clear();
-    int kind = -1, nrhs = -1;
-    for (auto it = sv->queue.begin(); it != sv->queue.end() && (int)batch.size() < sv->max_batch;) {
+    auto head = batch_head(sv);
+    if (head == sv->queue.end()) return;
+    const int kind = head->kind, nrhs = head->nrhs;
+    for (auto it = head; it != sv->queue.end() && (int)batch.size() < sv->max_batch;) {
         ServeSystem *s = sv->systems[it->sys];
-        if (!s->busy && batchable(sv, *it) && s->pk >= 0 &&
-            (kind < 0 || (it->kind == kind && it->nrhs == nrhs))) {
-            kind = it->kind;
-            nrhs = it->nrhs;
+        if (!s->busy && s->pk >= 0 && batchable(sv, *it) && it->kind == kind && it->nrhs == nrhs) {
             s->busy = true;
             batch.push_back(*it);
             it = sv->queue.erase(it);
@@ -363,12 +406,7 @@ static void take_batch(ServeState *sv, std::vector<ServeRequest> &batch)
     }
 }
 
-static bool has_batch_work(ServeState *sv)
-{
-    for (const ServeRequest &r : sv->queue)
-        if (!sv->systems[r.sys]->busy && batchable(sv, r)) return true;
-    return false;
-}
+static bool has_batch_work(ServeState *sv) { return batch_head(sv) != sv->queue.end(); }
 
 // One batch on lane `lane`: copy the inputs in, one packed product or one
 // lockstep block Lanczos over the batch's systems, copy the outputs out.
@@ -454,6 +492,7 @@ void serve_batch_loop(ServeState *sv, int lane)
             if (batch.empty()) continue;
             bl.busy = true;
         }
+        sv->cv.notify_all();  // workers may take partnered requests while no lane is free
         const int st = run_batch(sv, bl, batch);
         const double t_done = now_ms();
         {

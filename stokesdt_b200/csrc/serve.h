@@ -67,6 +67,7 @@ struct ServeState {
     std::vector<ServeWorker> workers;
     // continuous batching (monodisperse systems with K <= 256)
     bool batching = true;            // cleared by STOKESDT_SERVE_BATCH=0
+    bool batch_all = false;          // STOKESDT_SERVE_BATCH=all: lone requests to the batch lanes too
     int max_iters = 0, max_batch = 32;
     double tol = 0.0;
     std::vector<ServeBatchLane> blanes;
@@ -74,6 +75,7 @@ struct ServeState {
     bool pk_dirty = false, rebuilding = false;
     size_t lane_bytes = 0;           // device memory of the batch lanes' workspaces
     int lanes_active = 0;            // batch lanes whose workspace fits the budget
+    int workers_busy = 0;            // per-request workers running a request
     long long batches = 0, batched_requests = 0;
     std::deque<ServeRequest> queue;
     std::map<long long, int> status;

@@ -89,3 +89,38 @@ def test_batch_systems_shard_over_ranks():
     assert not set(m0) & set(m1) and sorted(m0 + m1) == list(range(32))
     assert t0 == t1 == 11.0
     assert max(c0, c1) < 0.6 * (c0 + c1) + 1e-3
+
+
+def _serve_worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    import bench
+    from stokesdt_b200 import workloads as wl
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    systems = bench.serve_systems(world)
+    mine = wl.shard_systems(systems, world, rank)
+    reqs = bench.serve_requests(len(systems), 60, 40.0, seed=3)
+    share = bench.rank_share(reqs, mine)
+    lat = bench.gather_all(dist, [float(i) for i in range(len(share))], world)
+    span = bench.max_over_ranks(dist, 1.0 + rank, "cpu")
+    out[rank] = (sorted(mine), len(systems), [tuple(r) for r in share], len(lat), span)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_serve_stream_shards_over_ranks():
+    """Config 5 over 2 ranks: 12 systems per rank, disjoint shards, every
+    request of the stream served by exactly one rank (the one owning its
+    system), latencies gathered over the whole job, span of the slowest."""
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    port = _free_port()
+    mp.spawn(_serve_worker, args=(2, port, out), nprocs=2, join=True)
+    (m0, n0, q0, l0, t0), (m1, n1, q1, l1, t1) = out[0], out[1]
+    assert n0 == n1 == 24
+    assert not set(m0) & set(m1) and sorted(m0 + m1) == list(range(24))
+    assert len(q0) + len(q1) == 60 and not set(q0) & set(q1)
+    assert all(r[1] in m0 for r in q0) and all(r[1] in m1 for r in q1)
+    assert l0 == l1 == 60
+    assert t0 == t1 == 2.0

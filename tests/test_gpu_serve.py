@@ -81,12 +81,15 @@ def test_admission_by_hbm_budget(gpu_available):
     srv.close()
 
 
-def test_mix_formed_while_a_batch_is_in_flight(gpu_available):
-    """Continuous batching: a Brownian batch (k = 16 on every system) is in
-    flight when mobility applies on the same systems arrive; they wait for
-    their systems and run together as later batches.  Every result equals the
-    same request served alone on a fresh server (1e-6 for M.f, 1e-5 for
-    sqrt(M) z), and the batches held more than one request each on average."""
+def test_mix_formed_while_a_batch_is_in_flight(gpu_available, monkeypatch):
+    """Continuous batching (STOKESDT_SERVE_BATCH=all: every batchable request
+    goes to the batch lanes, so the batch counts do not depend on thread
+    timing): a Brownian batch (k = 16 on every system) is in flight when
+    mobility applies on the same systems arrive; they wait for their systems
+    and run together as later batches.  Every result equals the same request
+    served alone on a fresh server in the default mode (1e-6 for M.f, 1e-5
+    for sqrt(M) z), and the batches held more than one request each on
+    average."""
     import stokesdt_b200 as sdt
     sy = _systems()
 
@@ -106,7 +109,9 @@ def test_mix_formed_while_a_batch_is_in_flight(gpu_available):
         n3 = 3 * s["npos"]
         inputs.append((i, 0, 4, rng.standard_normal((4, n3))))
         inputs.append((i, 0, 1, rng.standard_normal((1, n3))))
+    monkeypatch.setenv("STOKESDT_SERVE_BATCH", "all")
     srv, ids = server()
+    monkeypatch.delenv("STOKESDT_SERVE_BATCH")
     outs, tickets = [], []
     for (i, kind, k, x) in inputs:
         out = np.zeros_like(x)
@@ -126,3 +131,46 @@ def test_mix_formed_while_a_batch_is_in_flight(gpu_available):
         srv.wait(srv.submit(ids[i], kind, k, x, ref))
         srv.close()
         assert rel_err(ref, out) < (1e-6 if kind == 0 else 1e-5), (i, kind, k)
+
+
+def test_default_mode_routes_lone_and_batched_requests(gpu_available):
+    """Default continuous batching: requests with a partner (same kind and k
+    on another idle system) run as batches, lone ones on the per-request
+    workers.  Whatever the split, every request completes once and equals
+    the direct engine calls."""
+    import stokesdt_b200 as sdt
+    sy = _systems()
+    srv = sdt.MobilityServer(hbm_budget_bytes=20e9, lanes=1, max_npos=2000, max_iters=100, max_nrhs=16, tol=1e-6)
+    ids = [srv.register(s["npos"], np.ones(s["npos"]), s["box"], s["K"], s["xi"], s["rmax"], 6, s["pos"])
+           for s in sy]
+    rng = np.random.default_rng(5)
+    reqs = []
+    for rep in range(4):
+        for i, s in enumerate(sy):
+            n3 = 3 * s["npos"]
+            kind, k = (1, 4) if rep % 2 else (0, 4)
+            x = rng.standard_normal((k, n3))
+            out = np.zeros((k, n3))
+            reqs.append((i, kind, k, x, out, srv.submit(ids[i], kind, k, x, out)))
+    for r in reqs:
+        srv.wait(r[-1])
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["batched_requests"] <= len(reqs)
+    srv.close()
+    for i, s in enumerate(sy):
+        m = sdt.MobSpme(s["npos"], np.ones(s["npos"]), s["box"], s["xi"], s["rmax"], s["K"], 6)
+        assert m.Init()
+        m.Update(s["pos"])
+        lz = sdt.BrwnLanczos(3 * s["npos"], 100, 16, 1e-6, reorth=True)
+        assert lz.Init()
+        for (j, kind, k, x, out, _) in reqs:
+            if j != i:
+                continue
+            n3 = 3 * s["npos"]
+            ref = np.zeros((k, n3))
+            if kind == 0:
+                m.MulVector(k, 1.0, n3, x, 0.0, n3, ref)
+                assert rel_err(ref, out) < 1e-6
+            else:
+                lz.Compute(m, k, n3, x, n3, ref)
+                assert rel_err(ref, out) < 1e-5

@@ -21,6 +21,7 @@
  *                          (BrwnBase::Compute src/brwn/brwn_base.h:44-46)
  *   sdt_lanczos_destroy    BrwnLanczos::~BrwnLanczos           src/brwn/brwn_lanczos.cc:217-221
  *   sdt_bd_advance         BDSimBox::Advance step loop         src/simbox/simbox_bd.cc:296-366
+ *   sdt_bd_create[_ewald]  BDSimBox::InitMob / InitBrwn        src/simbox/simbox_bd.cc:89-184
  *   sdt_ewald_create       MobEwald::MobEwald + MobEwald::Init src/mob/mob_ewald.cc:21-108
  *   sdt_ewald_update       MobEwald::Update (EwaldKernel)      src/mob/mob_ewald.cc:111-127,
  *                          src/mob/ewald.cc:86-330 (tables :643-797)
@@ -368,6 +369,12 @@ typedef struct sdt_bd sdt_bd;
  * reference only logs it) and the step goes on with the last iterate. */
 int sdt_bd_create(sdt_spme *mob, sdt_lanczos *brwn, sdt_steric *steric, double dt, int mob_interval,
                   unsigned long long seed, sdt_bd **out);
+
+/* The same loop with the dense Ewald matrix as the mobility (MobEwald, the
+ * reference driver's default mob-method, src/simbox/simbox_bd.cc:93-103):
+ * Update rebuilds the matrix from the positions every mob_interval steps. */
+int sdt_bd_create_ewald(sdt_ewald *mob, sdt_lanczos *brwn, sdt_steric *steric, double dt, int mob_interval,
+                        unsigned long long seed, sdt_bd **out);
 
 /* Positions (3*npos, host); set resets nothing else. */
 int sdt_bd_set_positions(sdt_bd *h, const double *pos);

@@ -66,6 +66,8 @@ SIGNATURES = {
     "sdt_spme_synchronize": (ctypes.c_int, [_vp]),
     "sdt_bd_create": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
                                      ctypes.POINTER(_vp)]),
+    "sdt_bd_create_ewald": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
+                                           ctypes.POINTER(_vp)]),
     "sdt_bd_set_positions": (ctypes.c_int, [_vp, _dp]),
     "sdt_bd_get_positions": (ctypes.c_int, [_vp, _dp]),
     "sdt_bd_set_step": (ctypes.c_int, [_vp, ctypes.c_longlong]),
@@ -563,16 +565,18 @@ class BrwnLanczos:
 
 class BDIntegrator:
     """Device-resident BD step loop (the reference's BDSimBox::Advance,
-    src/simbox/simbox_bd.cc:296-366) over a MobSpme, a BrwnLanczos and an
-    optional StericForce of this package (all Init()-ed, same device)."""
+    src/simbox/simbox_bd.cc:296-366) over a MobSpme or a MobEwald, a
+    BrwnLanczos and an optional StericForce of this package (all Init()-ed,
+    same device)."""
 
-    def __init__(self, mob: MobSpme, brwn: BrwnLanczos, steric=None, dt=1e-3, mob_interval=16,
-                 seed=0):
+    def __init__(self, mob, brwn: BrwnLanczos, steric=None, dt=1e-3, mob_interval=16, seed=0):
         self.mob, self.brwn, self.steric = mob, brwn, steric
         self.npos = mob.npos
         h = _vp()
-        st = lib().sdt_bd_create(mob.handle, brwn._h, steric._h if steric is not None else None,
-                                 float(dt), int(mob_interval), int(seed), ctypes.byref(h))
+        create = lib().sdt_bd_create_ewald if isinstance(mob, MobEwald) else lib().sdt_bd_create
+        st = create(mob.handle if isinstance(mob, MobSpme) else mob._h, brwn._h,
+                    steric._h if steric is not None else None, float(dt), int(mob_interval), int(seed),
+                    ctypes.byref(h))
         if st != 0:
             raise StokesError(st, "sdt_bd_create failed")
         self._h = h

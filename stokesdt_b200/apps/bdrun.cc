@@ -5,14 +5,16 @@
 //   bdrun --config run.cfg --model run.mod --xyz start.xyz -n NSTEPS
 //
 // Config keys (defaults as BDSimBox): delta-t 0.001, mob-method
-// (spme | spme-gpu), brownian-method (lanczos | lanczos-gpu), mob-interval
-// 100, spme-nfft-grids 128, spme-porder 4, spme-xi 0.5, spme-rmax 4.0,
+// (ewald | ewald-gpu | spme | spme-gpu; default ewald), ewald-tol 1e-4,
+// brownian-method (lanczos | lanczos-gpu), mob-interval 100,
+// spme-nfft-grids 128, spme-porder 4, spme-xi 0.5, spme-rmax 4.0,
 // lanczos-maxiters 50, lanczos-maxnrhs 20, lanczos-tol 1e-3, traj-startstep
 // 0, traj-interval -1, traj-output trajectory.xyz, random-seed 1234.
 // The model file's par lines give the radii, its steric line the steric
-// force.  Positions, forces and random vectors stay on the GPU; frames are
-// written in the reference's XYZ layout.  The dense Ewald and Cholesky
-// methods of the reference are not offered (they are not on the GPU path).
+// force.  Positions, forces and random vectors stay on the GPU (the dense
+// Ewald matrix too: 72 N^2 bytes); frames are written in the reference's
+// XYZ layout.  The reference's Cholesky and random Brownian methods are not
+// offered (not on the GPU path).
 #include <getopt.h>
 
 #include <chrono>
@@ -83,8 +85,10 @@ int main(int argc, char **argv)
     }
     const std::string mob_method = cfg_str(cfg, "mob-method", "ewald");
     const std::string brwn_method = cfg_str(cfg, "brownian-method", "cholesky");
-    if (mob_method != "spme" && mob_method != "spme-gpu") {
-        std::fprintf(stderr, "mob-method %s: only spme / spme-gpu run on the GPU path\n", mob_method.c_str());
+    const bool ewald = mob_method == "ewald" || mob_method == "ewald-gpu";
+    if (!ewald && mob_method != "spme" && mob_method != "spme-gpu") {
+        std::fprintf(stderr, "mob-method %s: only ewald / spme (and their -gpu names) run on the GPU path\n",
+                     mob_method.c_str());
         return 1;
     }
     if (brwn_method != "lanczos" && brwn_method != "lanczos-gpu") {
@@ -131,25 +135,35 @@ int main(int argc, char **argv)
     const int has_steric = sdt_model_steric(model, &r0, &k0) == 0;
 
     sdt_spme *mob = nullptr;
+    sdt_ewald *ew = nullptr;
     sdt_lanczos *lz = nullptr;
     sdt_steric *st = nullptr;
     sdt_bd *bd = nullptr;
-    int rc = sdt_spme_create(npos, rdi.data(), box[0], xi, rmax, K, porder, device, &mob);
+    const double ewald_tol = cfg_f(cfg, "ewald-tol", 1e-4);
+    int rc = ewald ? sdt_ewald_create(npos, rdi.data(), box[0], ewald_tol, 0.0, device, &ew)
+                   : sdt_spme_create(npos, rdi.data(), box[0], xi, rmax, K, porder, device, &mob);
     if (rc != SDT_OK) {
-        std::fprintf(stderr, "SPME set-up failed (status %d): check spme-* keys\n", rc);
+        std::fprintf(stderr, "%s set-up failed (status %d): check the %s keys\n", ewald ? "Ewald" : "SPME", rc,
+                     ewald ? "ewald-*" : "spme-*");
         return 1;
     }
     rc = sdt_lanczos_create(3 * npos, max_iters, max_nrhs, tol, device, &lz);
     if (rc == SDT_OK && has_steric) rc = sdt_steric_create(npos, rdi.data(), box[0], r0, k0, device, &st);
-    if (rc == SDT_OK) rc = sdt_bd_create(mob, lz, st, dt, mob_interval, seed, &bd);
+    if (rc == SDT_OK)
+        rc = ewald ? sdt_bd_create_ewald(ew, lz, st, dt, mob_interval, seed, &bd)
+                   : sdt_bd_create(mob, lz, st, dt, mob_interval, seed, &bd);
     if (rc == SDT_OK) rc = sdt_bd_set_positions(bd, pos.data());
     if (rc == SDT_OK) rc = sdt_bd_set_step(bd, start_step);
     if (rc != SDT_OK) {
         std::fprintf(stderr, "set-up failed (status %d)\n", rc);
         return 1;
     }
-    std::printf("bdrun: %d particles, box %g, K %d, p %d, xi %g, rmax %g, dt %g, mob-interval %d, steric %s\n",
-                npos, box[0], K, porder, xi, rmax, dt, mob_interval, has_steric ? "on" : "off");
+    if (ewald)
+        std::printf("bdrun: %d particles, box %g, dense Ewald (tol %g), dt %g, mob-interval %d, steric %s\n", npos,
+                    box[0], ewald_tol, dt, mob_interval, has_steric ? "on" : "off");
+    else
+        std::printf("bdrun: %d particles, box %g, K %d, p %d, xi %g, rmax %g, dt %g, mob-interval %d, steric %s\n",
+                    npos, box[0], K, porder, xi, rmax, dt, mob_interval, has_steric ? "on" : "off");
     const auto t0 = std::chrono::steady_clock::now();
     long long istep = start_step;
     double time = start_time;
@@ -177,5 +191,6 @@ int main(int argc, char **argv)
     sdt_steric_destroy(st);
     sdt_lanczos_destroy(lz);
     sdt_spme_destroy(mob);
+    sdt_ewald_destroy(ew);
     return rc == SDT_OK ? 0 : 1;
 }

@@ -6,8 +6,10 @@
 //   irhs == 0:  Z <- N(0,1) [interval x 3N];  mob.Update(pos);
 //               Y <- sqrt(M) Z (block Lanczos, groups of max_nrhs)
 //   f <- 0; f += steric(pos)                           (forces, optional)
-//   Y[irhs] <- dt * M f + sqrt(2 dt) * Y[irhs]         (MobSpme::MulVector)
+//   Y[irhs] <- dt * M f + sqrt(2 dt) * Y[irhs]         (mob.MulVector)
 //   pos += Y[irhs]
+// with M the SPME operator (MobSpme) or the dense Ewald matrix (MobEwald,
+// the reference driver's default mob-method).
 //
 // Random vectors: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel
 // random numbers: as easy as 1, 2, 3", SC11) with key = seed and counter =
@@ -113,16 +115,19 @@ int bd_gaussian(cudaStream_t s, long long nvec, int dim, int ld, unsigned long l
 
 int bd_create(BdState *b)
 {
-    if (!b->mob || !b->lz) return bd_error(b, kErrInvalid, "mobility and Lanczos handles are required");
+    if ((!b->mob == !b->ew) || !b->lz)
+        return bd_error(b, kErrInvalid, "one mobility handle (SPME or Ewald) and a Lanczos handle are required");
     if (!(b->dt > 0.0)) return bd_error(b, kErrInvalid, "dt must be > 0");
     if (b->interval <= 0) return bd_error(b, kErrInvalid, "mob_interval must be > 0");
-    if (b->lz->dim != 3 * b->mob->npos) return bd_error(b, kErrInvalid, "Lanczos dimension != 3*npos");
-    if (b->steric && b->steric->npos != b->mob->npos)
+    const int npos = b->mob ? b->mob->npos : b->ew->npos;
+    const int device = b->mob ? b->mob->device : b->ew->device;
+    if (b->lz->dim != 3 * npos) return bd_error(b, kErrInvalid, "Lanczos dimension != 3*npos");
+    if (b->steric && b->steric->npos != npos)
         return bd_error(b, kErrInvalid, "steric force has a different particle count");
-    if (b->lz->device != b->mob->device || (b->steric && b->steric->device != b->mob->device))
+    if (b->lz->device != device || (b->steric && b->steric->device != device))
         return bd_error(b, kErrInvalid, "all handles must be on one device");
-    b->device = b->mob->device;
-    b->npos = b->mob->npos;
+    b->device = device;
+    b->npos = npos;
     b->ld = (3 * b->npos + 31) / 32 * 32;
     BD_CUDA(cudaSetDevice(b->device));
     BD_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
@@ -143,9 +148,11 @@ int bd_advance(BdState *b, int nsteps)
     const int n3 = 3 * b->npos;
     const double sq = std::sqrt(2.0 * b->dt);
     // every engine runs on the integrator's stream while it advances
-    cudaStream_t s_mob = b->mob->stream, s_lz = b->lz->stream;
+    cudaStream_t &mob_stream = b->mob ? b->mob->stream : b->ew->stream;
+    cudaStream_t s_mob = mob_stream, s_lz = b->lz->stream;
     cudaStream_t s_st = b->steric ? b->steric->stream : nullptr;
-    b->mob->stream = b->stream;
+    mob_stream = b->stream;
+    const std::string &mob_error = b->mob ? b->mob->last_error : b->ew->last_error;
     b->lz->stream = b->stream;
     if (b->steric) b->steric->stream = b->stream;
     int st = kOk;
@@ -157,14 +164,17 @@ int bd_advance(BdState *b, int nsteps)
                 bd_error(b, st, "random vectors: launch failed");
                 break;
             }
-            st = spme_update(b->mob, b->d_pos);
+            st = b->mob ? spme_update(b->mob, b->d_pos) : ewald_update(b->ew, b->d_pos);
             if (st != kOk) {
-                bd_error(b, st, "Update: " + b->mob->last_error);
+                bd_error(b, st, "Update: " + mob_error);
                 break;
             }
             const int ngroups = (b->interval + b->lz->max_nrhs - 1) / b->lz->max_nrhs;
             b->iters.assign(ngroups, 0);
-            st = lanczos_compute(b->lz, b->mob, b->interval, b->ld, b->d_z, b->ld, b->d_disp, b->iters.data());
+            st = b->mob ? lanczos_compute(b->lz, b->mob, b->interval, b->ld, b->d_z, b->ld, b->d_disp,
+                                          b->iters.data())
+                        : lanczos_compute_op(b->lz, ewald_mob_op(b->ew), b->interval, b->ld, b->d_z, b->ld,
+                                             b->d_disp, b->iters.data());
             if (st == kErrNotConverged) {
                 // BrwnLanczos only logs non-convergence; keep the last iterate
                 b->not_converged++;
@@ -186,9 +196,10 @@ int bd_advance(BdState *b, int nsteps)
                 break;
             }
         }
-        st = spme_mulvec(b->mob, 0, 1, b->dt, b->ld, b->d_f, sq, b->ld, disp);
+        st = b->mob ? spme_mulvec(b->mob, 0, 1, b->dt, b->ld, b->d_f, sq, b->ld, disp)
+                    : ewald_mulvec(b->ew, 1, b->dt, b->ld, b->d_f, sq, b->ld, disp);
         if (st != kOk) {
-            bd_error(b, st, "MulVector: " + b->mob->last_error);
+            bd_error(b, st, "MulVector: " + mob_error);
             break;
         }
         k_bd_axpy<<<(n3 + 255) / 256, 256, 0, b->stream>>>(n3, disp, b->d_pos);
@@ -199,7 +210,7 @@ int bd_advance(BdState *b, int nsteps)
         }
         b->istep++;
     }
-    b->mob->stream = s_mob;
+    mob_stream = s_mob;
     b->lz->stream = s_lz;
     if (b->steric) b->steric->stream = s_st;
     return st;

@@ -6,13 +6,15 @@
 #include <vector>
 
 #include "engine.h"
+#include "ewald.h"
 #include "lanczos.h"
 #include "steric.h"
 
 namespace sdt {
 
 struct BdState {
-    SpmeEngine *mob = nullptr;
+    SpmeEngine *mob = nullptr;       // the mobility: SPME, or
+    EwaldEngine *ew = nullptr;       // the dense Ewald matrix (exactly one of the two)
     LanczosState *lz = nullptr;
     StericEngine *steric = nullptr;  // optional
     int device = 0;

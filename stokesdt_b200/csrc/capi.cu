@@ -383,6 +383,29 @@ int sdt_bd_create(sdt_spme *mob, sdt_lanczos *brwn, sdt_steric *steric, double d
     return SDT_OK;
 }
 
+int sdt_bd_create_ewald(sdt_ewald *mob, sdt_lanczos *brwn, sdt_steric *steric, double dt, int mob_interval,
+                        unsigned long long seed, sdt_bd **out)
+{
+    if (!out) return SDT_ERR_INVALID;
+    *out = nullptr;
+    sdt_bd *h = new (std::nothrow) sdt_bd;
+    if (!h) return SDT_ERR_ALLOC;
+    h->s.ew = mob ? &mob->e : nullptr;
+    h->s.lz = brwn ? &brwn->s : nullptr;
+    h->s.steric = steric ? &steric->e : nullptr;
+    h->s.dt = dt;
+    h->s.interval = mob_interval;
+    h->s.seed = seed;
+    const int st = sdt::bd_create(&h->s);
+    if (st != SDT_OK) {
+        sdt::bd_free(&h->s);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return SDT_OK;
+}
+
 int sdt_bd_set_positions(sdt_bd *h, const double *pos)
 {
     if (!h || !pos) return SDT_ERR_INVALID;
@@ -887,22 +910,6 @@ void sdt_ewald_destroy(sdt_ewald *h)
     delete h;
 }
 
-namespace {
-sdt::MobOp ewald_op(sdt::EwaldEngine *e)
-{
-    sdt::MobOp op;
-    op.dim = e->n3;
-    op.mulvec = [e](int nr, double a, int ldf, const double *f, double b, int ldv, double *v, cudaStream_t s) {
-        cudaStream_t saved = e->stream;
-        e->stream = s;
-        const int st = sdt::ewald_mulvec(e, nr, a, ldf, f, b, ldv, v);
-        e->stream = saved;
-        return st;
-    };
-    op.error = [e]() { return e->last_error; };
-    return op;
-}
-}  // namespace
 
 int sdt_lanczos_compute_ewald_device(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz, const double *d_z, int ldy,
                                      double *d_y, int *iters)
@@ -912,7 +919,7 @@ int sdt_lanczos_compute_ewald_device(sdt_lanczos *h, sdt_ewald *mob, int nrhs, i
     if (cudaSetDevice(lz->device) != cudaSuccess) return SDT_ERR_CUDA;
     // the matrix is built on the engine stream: the solver's stream waits for it
     if (cudaStreamSynchronize(mob->e.stream) != cudaSuccess) return SDT_ERR_CUDA;
-    const int st = sdt::lanczos_compute_op(lz, ewald_op(&mob->e), nrhs, ldz, d_z, ldy, d_y, iters);
+    const int st = sdt::lanczos_compute_op(lz, sdt::ewald_mob_op(&mob->e), nrhs, ldz, d_z, ldy, d_y, iters);
     if (cudaStreamSynchronize(lz->stream) != cudaSuccess) return SDT_ERR_CUDA;
     return st;
 }
@@ -949,7 +956,7 @@ int sdt_lanczos_compute_ewald(sdt_lanczos *h, sdt_ewald *mob, int nrhs, int ldz,
         return SDT_ERR_CUDA;
     }
     if (cudaStreamSynchronize(mob->e.stream) != cudaSuccess) return SDT_ERR_CUDA;
-    const int st = sdt::lanczos_compute_op(lz, ewald_op(&mob->e), nrhs, n, lz->d_zin, n, lz->d_yout, iters);
+    const int st = sdt::lanczos_compute_op(lz, sdt::ewald_mob_op(&mob->e), nrhs, n, lz->d_zin, n, lz->d_yout, iters);
     if (st != SDT_OK && st != SDT_ERR_NOT_CONVERGED) return st;
     if (cudaMemcpy2DAsync(y, (size_t)ldy * sizeof(double), lz->d_yout, row, row, nrhs, cudaMemcpyDeviceToHost,
                           lz->stream) != cudaSuccess ||

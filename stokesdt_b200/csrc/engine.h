@@ -141,7 +141,7 @@ struct SpmeEngine {
     // z pass with forward FFT, influence and inverse FFT fused in registers
     // (K <= 256, TMA path; cleared by STOKESDT_NO_ZFUSE=1)
     bool zfused = true;
-    // tensor-core spread (K = 256, calls of >= kTcRhsPerCta RHS; cleared by
+    // tensor-core spread (K = 256, calls of >= kTcMinRhs RHS; cleared by
     // STOKESDT_NO_TC=1, and for batch and served engines): per 2x2 row block
     // the particles whose support reaches it (padded to whole 16-particle
     // chunks), their 4 row weights wz*wy and their x-transformed weight
@@ -197,9 +197,9 @@ int pair_list_build(SpmeEngine *e);
 void pair_list_free(SpmeEngine *e);
 
 int set_error(SpmeEngine *e, int status, const std::string &msg);
-// Right-hand sides one tensor-core spread CTA takes; calls with fewer use the
-// shared-memory spread.
-constexpr int kTcRhsPerCta = 8;
+// Fewest right-hand sides of a call that takes the tensor-core spread; calls
+// with fewer use the shared-memory spread.
+constexpr int kTcMinRhs = 8;
 int tc_build(SpmeEngine *e);
 void tc_free(SpmeEngine *e);
 int spread_tc_launch(SpmeEngine *e, int nr, int r0, cudaStream_t s);

@@ -362,4 +362,19 @@ void ewald_free(EwaldEngine *e)
     *e = EwaldEngine();
 }
 
+MobOp ewald_mob_op(EwaldEngine *e)
+{
+    MobOp op;
+    op.dim = e->n3;
+    op.mulvec = [e](int nr, double a, int ldf, const double *f, double b, int ldv, double *v, cudaStream_t s) {
+        cudaStream_t saved = e->stream;
+        e->stream = s;
+        const int st = ewald_mulvec(e, nr, a, ldf, f, b, ldv, v);
+        e->stream = saved;
+        return st;
+    };
+    op.error = [e]() { return e->last_error; };
+    return op;
+}
+
 }  // namespace sdt

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "lanczos.h"
 
 namespace sdt {
 
@@ -38,5 +39,8 @@ int ewald_update(EwaldEngine *e, const double *d_pos);
 int ewald_mulvec(EwaldEngine *e, int nrhs, double alpha, int ldf, const double *d_f, double beta, int ldv,
                  double *d_v);
 void ewald_free(EwaldEngine *e);
+// The engine as a mobility operator for the block Lanczos (products queued on
+// the stream the solver passes).
+MobOp ewald_mob_op(EwaldEngine *e);
 
 }  // namespace sdt

@@ -1271,7 +1271,7 @@ static int recip_pass(SpmeEngine *e, int nr, const float *tab, const double *isc
         return set_error(e, kErrUnsupported, "the forward-spectrum diagnostic needs the fused z pass (K <= 256)");
     const int ty = kTileX * FftShape<K>::N2;
     const int tz = 3 * kTileZ * FftShape<K>::N2;
-    if (K == 256 && e->tc_ready && nr >= kTcRhsPerCta) {
+    if (K == 256 && e->tc_ready && nr >= kTcMinRhs) {
         const int st = spread_tc_launch(e, nr, r0, s);
         if (st != kOk) return st;
     } else {

@@ -7,9 +7,9 @@
 //   Bx_p(kx) = sum_j wx_p(j) exp(-2 pi i kx (x0_p + j) / K)
 // (the x B-spline weights transformed once per Update).  The 256 real values
 // Re Bx(0..H), Im Bx(1..H-1) of a particle form one GEMM column; with M =
-// those 256 values (two 128-row MMA tiles), N = 8 RHS x 3 components x 4
-// rows = 96
-// and K = the block's particles in chunks of 16, tcgen05.mma (kind::tf32,
+// those 256 values (two 128-row MMA tiles), N = up to 16 RHS x 3 components
+// x 4 rows = 192 and K = the block's particles in chunks of 16, tcgen05.mma
+// (kind::tf32,
 // FP32 accumulation in tensor memory) computes the block's half spectra
 // directly: no shared-memory atomics and no x FFT.  FP32 accuracy comes from
 // the 3-term TF32 split a*b ~ ah*bh + ah*bl + al*bh (relative error ~1e-7 on
@@ -34,9 +34,6 @@ namespace {
 constexpr int kTcChunk = 16;                               // particles per MMA K chunk
 constexpr int kTcBY = 2, kTcBZ = 2;                        // rows of a block along y, z
 constexpr int kTcRows = kTcBY * kTcBZ;                     // rows of a block (4)
-constexpr int kTcRhs = kTcRhsPerCta;                       // right-hand sides per CTA
-constexpr int kTcCols = kTcRhs * 3 * kTcRows;              // N of the MMA (96)
-constexpr int kTcThreads = 256;
 
 // Blocks a particle's support reaches: z pieces x y pieces.
 constexpr int kTcMaxParts = 5;  // pieces of p <= 8 consecutive rows in blocks of 2
@@ -131,218 +128,301 @@ __global__ void k_tc_bx(long long nent, int p, const int *__restrict__ slot, con
     tile[K * kTcChunk + off] = lo;
 }
 
-// One CTA per (RHS, row block), two pipeline stages of one chunk each:
-// while chunk c is staged and its MMAs run, the bulk copy of chunk c + 1 is
-// in flight into the other stage (issued as soon as the MMAs of chunk c - 1
-// have released that stage).  Per chunk: form the force x row-weight operand
-// (hi/lo), issue 3 x (kTcChunk / 8) x (K / 128) MMAs, commit to the stage's
-// barrier.  Then write the 96 half-spectrum rows from tensor memory.
-template <int K>
-__global__ void __launch_bounds__(kTcThreads, 2)
-k_spread_tc(int n, int nby, const int *__restrict__ tc_start, const int *__restrict__ tc_slot,
+// Persistent, warp-specialised kernel: one CTA per SM walks the row blocks
+// blockIdx.x, blockIdx.x + gridDim.x, ...; every block's chunks run through
+// one pipeline whose stages are
+//   - the copy thread (warp 0): a chunk's Bx operand tiles (hi and lo) and
+//     row weights into a ring of kTcRing slots by bulk copy, as soon as the
+//     MMAs have released the slot;
+//   - the MMA thread (warp 1): per chunk 3 x (kTcChunk / 8) x (K / 128)
+//     tcgen05 MMAs with all NRHS right-hand sides in one accumulator
+//     (N = NRHS x 3 components x 4 rows), so each operand tile is read once
+//     per product; commits release the slot, the force operand buffer and,
+//     after a block's last chunk, the accumulator;
+//   - eight builder warps: the force x row-weight operand (hi / lo) of a
+//     chunk into one of two buffers (each thread builds the columns of the
+//     forces it gathered one chunk ahead), and after a block's last chunk the
+//     epilogue: tensor memory -> half-spectrum rows in HBM.
+// mbarriers connect the stages; every wait is bounded, and a wait that gives
+// up sets the error word and an abort flag that ends the other stages'
+// waits, so the CTA always reaches its final barrier and frees its tensor
+// memory after its copies and MMAs have landed.
+constexpr int kTcRing = 3;                          // chunks whose operand tiles are in flight
+constexpr int kTcBuildWarps = 8;
+constexpr int kTcBuilders = 32 * kTcBuildWarps;
+constexpr int kTcThreads = 64 + kTcBuilders;        // copy warp, MMA warp, builders
+
+// Bounded wait that also gives up once another stage has aborted.
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
+{
+    for (int i = 0; i < kMbarPollLimit; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255) == 255 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    return false;
+}
+
+template <int K, int NRHS>
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const int *__restrict__ tc_slot,
             const float *__restrict__ tc_w, const float *__restrict__ tc_bx, const float *__restrict__ fs_sp,
             int XS, float2 *__restrict__ cgrid, int r0, int nr, int *err)
 {
     static_assert(K == 256, "two 128-row tiles: Re Bx(0..127) | Re Bx(128), Im Bx(1..127)");
     constexpr int H = K / 2;
     constexpr int MT = K / 128;
-    constexpr int A_FL = K * kTcChunk;        // floats of one (hi or lo) Bx tile set
-    constexpr int B_FL = kTcCols * kTcChunk;  // floats of one (hi or lo) force operand
+    constexpr int NCOL = NRHS * 3 * kTcRows;      // N of the MMA
+    constexpr int A_FL = K * kTcChunk;            // floats of one (hi or lo) Bx tile set
     constexpr int W_FL = kTcChunk * kTcRows;
-    constexpr int F_FL = kTcRhs * 3 * kTcChunk;
-    constexpr int STAGE = 2 * A_FL + 2 * B_FL + W_FL + F_FL;  // floats per stage
+    constexpr int SLOT = 2 * A_FL + W_FL;         // ring slot: A hi | A lo | row weights
+    constexpr int B_FL = NCOL * kTcChunk;         // floats of one (hi or lo) force operand
+    constexpr int NF = NRHS * 3 * kTcChunk;       // forces of one chunk
+    constexpr int FPT = (NF + kTcBuilders - 1) / kTcBuilders;
     constexpr uint32_t kLbo = 128, kSbo = (kTcChunk / 4) * 128;
-    constexpr uint32_t kLoadBytes = (uint32_t)((2 * A_FL + W_FL) * sizeof(float));
-    extern __shared__ __align__(1024) float smf[];  // 2 stages of [A hi|A lo|B hi|B lo|W|F]
-    __shared__ uint64_t bar_ld[2], bar_mma[2];
+    constexpr uint32_t kLoadBytes = (uint32_t)(SLOT * sizeof(float));
+    constexpr uint32_t kAccStride = 256;          // tensor-memory columns between the two M tiles
+    constexpr uint32_t kTmemCols = 512;
+    static_assert(NCOL <= (int)kAccStride && NCOL % 16 == 0, "accumulator fits its half of tensor memory");
+    extern __shared__ __align__(1024) float smf[];  // [kTcRing][SLOT], then [2][B hi | B lo]
+    float *const ring = smf;
+    float *const opb = smf + kTcRing * SLOT;
+    __shared__ uint64_t ring_full[kTcRing], ring_empty[kTcRing], op_full[2], op_empty[2], acc_full, acc_empty;
     __shared__ uint32_t tmem_base;
-    const int by = blockIdx.x, bz = blockIdx.y;
+    __shared__ int abort_flag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int blk = bz * nby + by;
-    const int q0 = tc_start[blk], q1 = tc_start[blk + 1];
-    const int nch = (q1 - q0) / kTcChunk;
-    // the CTA takes every RHS group of its row block in turn, so each group
-    // after the first reads the block's operand tiles back from L2; steps
-    // s = g * nch + c run group g, chunk c through one pipeline
-    const int ngrp = (nr + kTcRhs - 1) / kTcRhs;
-    const int nsteps = nch * ngrp;
-    if (warp == 0) tc_alloc(&tmem_base, 256);
+    if (warp == 0) tc_alloc(&tmem_base, kTmemCols);
     if (tid == 0) {
-        for (int i = 0; i < 2; i++) {
-            mbar_init(&bar_ld[i], 1);
-            mbar_init(&bar_mma[i], 1);
+        for (int i = 0; i < kTcRing; i++) {
+            mbar_init(&ring_full[i], 1);
+            mbar_init(&ring_empty[i], 1);
         }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&op_full[i], kTcBuilders);
+            mbar_init(&op_empty[i], 1);
+        }
+        mbar_init(&acc_full, 1);
+        mbar_init(&acc_empty, kTcBuilders);
+        abort_flag = 0;
         fence_barrier_init();
     }
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
     const uint32_t tbase = tmem_base;
-    constexpr uint32_t idesc = tc_idesc_tf32(128, kTcCols);
-    auto issue_load = [&](int step) {
-        float *st = smf + (step & 1) * STAGE;
-        const int q = q0 + (step % nch) * kTcChunk;
-        mbar_arrive_expect_tx(&bar_ld[step & 1], kLoadBytes);
-        bulk_load(st, tc_bx + (size_t)(q / kTcChunk) * 2 * A_FL, (uint32_t)(2 * A_FL * sizeof(float)),
-                  &bar_ld[step & 1]);
-        bulk_load(st + 2 * A_FL + 2 * B_FL, tc_w + (size_t)q * kTcRows, (uint32_t)(W_FL * sizeof(float)),
-                  &bar_ld[step & 1]);
+    volatile int *abort = &abort_flag;
+    auto chunks = [&](int b, int &q0) {
+        q0 = tc_start[b];
+        return (tc_start[b + 1] - q0) / kTcChunk;
     };
-    if (tid == 0 && nsteps > 0) issue_load(0);
-    // forces of the next step, gathered one step ahead (slot -> force is two
-    // dependent loads; they overlap the current step's work); value
-    // t = tid + u * kTcThreads is RHS rl, component c, entry k with
-    // t = (rl * 3 + c) * kTcChunk + k
-    constexpr int FPT = (F_FL + kTcThreads - 1) / kTcThreads;
-    const int fk = tid % kTcChunk;
-    float fnext[FPT];
-    auto gather_forces = [&](int step) {
-        const int rb = (step / nch) * kTcRhs;
-        const int s = tc_slot[q0 + (step % nch) * kTcChunk + fk];
-#pragma unroll
-        for (int u = 0; u < FPT; u++) {
-            const int t = tid + u * kTcThreads, fcc = t / kTcChunk, frl = fcc / 3;
-            fnext[u] = (t < F_FL && rb + frl < nr && s >= 0)
-                           ? fs_sp[(size_t)(3 * (r0 + rb + frl) + fcc % 3) * n + s]
-                           : 0.0f;
+
+    if (warp == 0) {
+        // ---- copy thread
+        if (lane == 0) {
+            int step = 0;
+            bool ok = true;
+            for (int b = blockIdx.x; b < nblk && ok; b += gridDim.x) {
+                int q0;
+                const int nch = chunks(b, q0);
+                for (int c = 0; c < nch; c++, step++) {
+                    const int s = step % kTcRing, u = step / kTcRing;
+                    if (!tc_wait(&ring_empty[s], (u & 1) ^ 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    float *dst = ring + s * SLOT;
+                    const int q = q0 + c * kTcChunk;
+                    mbar_arrive_expect_tx(&ring_full[s], kLoadBytes);
+                    bulk_load(dst, tc_bx + (size_t)(q / kTcChunk) * 2 * A_FL, (uint32_t)(2 * A_FL * sizeof(float)),
+                              &ring_full[s]);
+                    bulk_load(dst + 2 * A_FL, tc_w + (size_t)q * kTcRows, (uint32_t)(W_FL * sizeof(float)),
+                              &ring_full[s]);
+                }
+            }
+            if (!ok) atomicExch(err, kTmaErrTimeout);
+            // every copy issued must land before the CTA ends (the last
+            // kTcRing copies are the only ones that may still be in flight)
+            for (int i = step > kTcRing ? step - kTcRing : 0; i < step; i++)
+                mbar_wait(&ring_full[i % kTcRing], (i / kTcRing) & 1);
         }
-    };
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---- MMA thread
+        if (lane == 0) {
+            constexpr uint32_t idesc = tc_idesc_tf32(128, NCOL);
+            int step = 0, j = 0;
+            bool ok = true;
+            for (int b = blockIdx.x; b < nblk && ok; b += gridDim.x) {
+                int q0;
+                const int nch = chunks(b, q0);
+                if (nch == 0) continue;
+                if (!tc_wait(&acc_empty, (j & 1) ^ 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after_sync();
+                for (int c = 0; c < nch; c++, step++) {
+                    const int s = step % kTcRing, u = step / kTcRing, ob = step & 1, v = step >> 1;
+                    if (!tc_wait(&ring_full[s], u & 1, abort) || !tc_wait(&op_full[ob], v & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after_sync();
+                    const float *sA = ring + s * SLOT;
+                    const float *sB = opb + ob * 2 * B_FL;
+                    for (int mt = 0; mt < MT; mt++) {
+                        const uint32_t d = tbase + (uint32_t)mt * kAccStride;
 #pragma unroll
-    for (int u = 0; u < FPT; u++) fnext[u] = 0.0f;
-    if (nsteps > 0) gather_forces(0);
-    // epilogue of RHS group g: thread (warp, lane) holds kx = 32 (warp % 4) +
-    // lane of tile 0 (Re) and tile 1 (Im; lane 0 of warps 0 and 4 holds
-    // Re Bx(H) instead); warps w and w + 4 read the same lanes and split the
-    // columns
-    auto epilogue = [&](int g, bool zero) {
-        const int rb = g * kTcRhs;
-        const int wq = warp & 3;
-        const int kx = wq * 32 + lane;
-        const uint32_t trow = tbase + ((uint32_t)(wq * 32) << 16);
-        constexpr int GPW = kTcCols / 16 / (kTcThreads / 128);  // column groups per warp
+                        for (int ks = 0; ks < kTcChunk / 8; ks++) {
+                            const float *ah = sA + mt * 128 * kTcChunk + ks * 64, *al = ah + A_FL;
+                            const float *bh = sB + ks * 64, *bl = bh + B_FL;
+                            const uint64_t dah = tc_smem_desc(ah, kLbo, kSbo), dal = tc_smem_desc(al, kLbo, kSbo);
+                            const uint64_t dbh = tc_smem_desc(bh, kLbo, kSbo), dbl = tc_smem_desc(bl, kLbo, kSbo);
+                            tc_mma_tf32(d, dah, dbh, idesc, !(c == 0 && ks == 0));
+                            tc_mma_tf32(d, dah, dbl, idesc, true);
+                            tc_mma_tf32(d, dal, dbh, idesc, true);
+                        }
+                    }
+                    tc_commit(&op_empty[ob]);
+                    tc_commit(&ring_empty[s]);
+                }
+                if (!ok) break;
+                tc_commit(&acc_full);
+                j++;
+            }
+            if (!ok) atomicExch(err, kTmaErrTimeout);
+            // the MMAs issued last must complete before the CTA ends
+            if (step > 0) mbar_wait(&op_empty[(step - 1) & 1], ((step - 1) >> 1) & 1);
+        }
+        __syncwarp();
+    } else {
+        // ---- builders: force operand per chunk, epilogue per block
+        const int bt = tid - 64;
+        const int q4 = warp & 3;                         // tensor-memory lane quarter of this warp
+        const int half = (warp - 2) >> 2;                // which half of the column groups it writes
+        // forces gathered for (component column cc, entry k) = (idx / 16, idx % 16), idx = bt + u * 256
+        auto gather = [&](int qc, float (&f)[FPT]) {
+#pragma unroll
+            for (int u = 0; u < FPT; u++) {
+                const int idx = bt + u * kTcBuilders;
+                f[u] = 0.0f;
+                if (idx < NF) {
+                    const int cc = idx / kTcChunk, k = idx % kTcChunk, rl = cc / 3;
+                    const int s = tc_slot[qc + k];
+                    if (rl < nr && s >= 0) f[u] = fs_sp[(size_t)(3 * (r0 + rl) + cc % 3) * n + s];
+                }
+            }
+        };
+        auto epilogue = [&](int b, bool zero) {
+            const int by = b % nby, bz = b / nby;
+            const int kx = q4 * 32 + lane;
+            const uint32_t trow = tbase + ((uint32_t)(q4 * 32) << 16);
+            constexpr int NG = NCOL / 16;
 #pragma unroll 1
-        for (int gg = (warp >> 2) * GPW; gg < ((warp >> 2) + 1) * GPW; gg++) {
-            float re[16], im[16];
-            if (!zero) {
-                tc_ld_32x16(trow + (uint32_t)(gg * 16), re);
-                tc_ld_32x16(trow + 128u + (uint32_t)(gg * 16), im);
-                tc_wait_ld();
-            } else {
+            for (int gg = half * (NG / 2); gg < (half + 1) * (NG / 2) + (half ? NG % 2 : 0); gg++) {
+                float re[16], im[16];
+                if (!zero) {
+                    tc_ld_32x16(trow + (uint32_t)(gg * 16), re);
+                    tc_ld_32x16(trow + kAccStride + (uint32_t)(gg * 16), im);
+                    tc_wait_ld();
+                } else {
 #pragma unroll
-                for (int j = 0; j < 16; j++) re[j] = im[j] = 0.0f;
-            }
+                    for (int jj = 0; jj < 16; jj++) re[jj] = im[jj] = 0.0f;
+                }
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const int col = gg * 16 + j;
-                const int cc = col / kTcRows, row = col % kTcRows, rl = cc / 3;
-                const int z = kTcBZ * bz + row / kTcBY, y = kTcBY * by + row % kTcBY;
-                float2 *gp = cgrid + (((size_t)(3 * (r0 + rb + rl) + cc % 3) * K + z) * K + y) * XS;
-                if (rb + rl < nr) {
-                    gp[kx] = make_float2(re[j], kx == 0 ? 0.0f : im[j]);
-                    if (kx == 0) gp[H] = make_float2(im[j], 0.0f);
+                for (int jj = 0; jj < 16; jj++) {
+                    const int col = gg * 16 + jj;
+                    const int cc = col / kTcRows, row = col % kTcRows, rl = cc / 3;
+                    const int z = kTcBZ * bz + row / kTcBY, y = kTcBY * by + row % kTcBY;
+                    float2 *gp = cgrid + (((size_t)(3 * (r0 + rl) + cc % 3) * K + z) * K + y) * XS;
+                    if (rl < nr) {
+                        gp[kx] = make_float2(re[jj], kx == 0 ? 0.0f : im[jj]);
+                        if (kx == 0) gp[H] = make_float2(im[jj], 0.0f);
+                    }
                 }
             }
-        }
-    };
-    bool ok = true;
-    int fail_bar = -1;  // 0..1: a load barrier, 2..3: an MMA barrier
-    int fail_par = 0;
-    for (int step = 0; step < nsteps; step++) {
-        const int sidx = step & 1, c = step % nch;
-        float *st = smf + sidx * STAGE;
-        float *sA = st, *sB = st + 2 * A_FL, *sW = sB + 2 * B_FL, *sF = sW + W_FL;
-        // the other stage is free once the MMAs of step - 1 are done: fetch
-        // step + 1 into it now.  The fetching thread is in the last warp, so
-        // the other warps go on with this step while it waits for those MMAs.
-        if (tid == kTcThreads - 32 && step + 1 < nsteps) {
-            if (step >= 1 && !mbar_wait(&bar_mma[sidx ^ 1], ((step - 1) >> 1) & 1)) {
-                ok = false;
-                fail_bar = 2 + (sidx ^ 1);
-                fail_par = ((step - 1) >> 1) & 1;
-            } else {
-                issue_load(step + 1);
+        };
+        float fcur[FPT], fnext[FPT];
+        // next chunk of the walk after (b, c): the same block's next chunk or
+        // the first chunk of the next non-empty block; false at the end
+        auto next_chunk = [&](int b, int c, int nch, int q0, int &qn) {
+            if (c + 1 < nch) {
+                qn = q0 + (c + 1) * kTcChunk;
+                return true;
             }
-        }
-#pragma unroll
-        for (int u = 0; u < FPT; u++)
-            if (tid + u * kTcThreads < F_FL) sF[tid + u * kTcThreads] = fnext[u];
-        if (step + 1 < nsteps) gather_forces(step + 1);
-        if (ok && !mbar_wait(&bar_ld[sidx], (step >> 1) & 1)) {
-            ok = false;
-            fail_bar = sidx;
-            fail_par = (step >> 1) & 1;
-        }
-        if (!__syncthreads_and(ok)) {
-            ok = false;
-            break;
-        }
-        // force operand: column ((rl, c), row), K index = entry k; a warp
-        // writes one 8-column x 4-entry core-matrix slab (32 consecutive floats)
-        for (int v = tid; v < kTcCols * kTcChunk; v += kTcThreads) {
-            const int g = v >> 5, l = v & 31;
-            const int k = (g % (kTcChunk / 4)) * 4 + (l & 3), col = (g / (kTcChunk / 4)) * 8 + (l >> 2);
-            const int cc = col / kTcRows, row = col % kTcRows;
-            const float x = sF[cc * kTcChunk + k] * sW[k * kTcRows + row];
-            const float hi = tf32_round(x), lo = tf32_round(x - hi);
-            const uint32_t off = tc_kmajor_offset(col, k, kTcChunk) / 4;
-            sB[off] = hi;
-            sB[B_FL + off] = lo;
-        }
-        fence_proxy_async_smem();
-        tc_fence_before_sync();
-        __syncthreads();
-        tc_fence_after_sync();
-        if (tid == 0) {
-            for (int mt = 0; mt < MT; mt++) {
-                const uint32_t d = tbase + (uint32_t)(mt * 128);
-#pragma unroll
-                for (int s = 0; s < kTcChunk / 8; s++) {
-                    const float *ah = sA + mt * 128 * kTcChunk + s * 64, *al = ah + A_FL;
-                    const float *bh = sB + s * 64, *bl = bh + B_FL;
-                    const uint64_t dah = tc_smem_desc(ah, kLbo, kSbo), dal = tc_smem_desc(al, kLbo, kSbo);
-                    const uint64_t dbh = tc_smem_desc(bh, kLbo, kSbo), dbl = tc_smem_desc(bl, kLbo, kSbo);
-                    tc_mma_tf32(d, dah, dbh, idesc, !(c == 0 && s == 0));
-                    tc_mma_tf32(d, dah, dbl, idesc, true);
-                    tc_mma_tf32(d, dal, dbh, idesc, true);
+            for (int b2 = b + (int)gridDim.x; b2 < nblk; b2 += gridDim.x) {
+                int q2;
+                if (chunks(b2, q2) > 0) {
+                    qn = q2;
+                    return true;
                 }
             }
-            tc_commit(&bar_mma[sidx]);
-        }
-        if (c == nch - 1) {
-            // last chunk of the group: wait for its MMAs, write the group's
-            // spectra, and release the accumulators for the next group
-            if (tid == 0 && !mbar_wait(&bar_mma[sidx], (step >> 1) & 1)) {
-                ok = false;
-                fail_bar = 2 + sidx;
-                fail_par = (step >> 1) & 1;
+            return false;
+        };
+        int first_q = -1;
+        for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+            int q0;
+            if (chunks(b, q0) > 0) {
+                first_q = q0;
+                break;
             }
-            if (!__syncthreads_and(ok)) {
+        }
+        if (first_q >= 0) gather(first_q, fnext);
+        int step = 0, j = 0;
+        bool ok = true;
+        for (int b = blockIdx.x; b < nblk && ok; b += gridDim.x) {
+            int q0;
+            const int nch = chunks(b, q0);
+            if (nch == 0) {
+                epilogue(b, true);
+                continue;
+            }
+            for (int c = 0; c < nch; c++, step++) {
+#pragma unroll
+                for (int u = 0; u < FPT; u++) fcur[u] = fnext[u];
+                int qn;
+                if (next_chunk(b, c, nch, q0, qn)) gather(qn, fnext);
+                const int s = step % kTcRing, u = step / kTcRing, ob = step & 1, v = step >> 1;
+                if (!tc_wait(&ring_full[s], u & 1, abort) || !tc_wait(&op_empty[ob], (v & 1) ^ 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                const float *sW = ring + s * SLOT + 2 * A_FL;
+                float *bh = opb + ob * 2 * B_FL, *bl = bh + B_FL;
+#pragma unroll
+                for (int uu = 0; uu < FPT; uu++) {
+                    const int idx = bt + uu * kTcBuilders;
+                    if (idx < NF) {
+                        const int cc = idx / kTcChunk, k = idx % kTcChunk;
+#pragma unroll
+                        for (int row = 0; row < kTcRows; row++) {
+                            const float x = fcur[uu] * sW[k * kTcRows + row];
+                            const float hi = tf32_round(x), lo = tf32_round(x - hi);
+                            const uint32_t off = tc_kmajor_offset(cc * kTcRows + row, k, kTcChunk) / 4;
+                            bh[off] = hi;
+                            bl[off] = lo;
+                        }
+                    }
+                }
+                fence_proxy_async_smem();
+                mbar_arrive(&op_full[ob]);
+            }
+            if (!ok) break;
+            if (!tc_wait(&acc_full, j & 1, abort)) {
                 ok = false;
                 break;
             }
             tc_fence_after_sync();
-            epilogue(step / nch, false);
+            epilogue(b, false);
             tc_fence_before_sync();
-            __syncthreads();
+            mbar_arrive(&acc_empty);
+            j++;
         }
+        if (!ok) atomicExch(err, kTmaErrTimeout);
     }
-    if (!ok) {
-        // a copy or MMAs did not complete in time: let them land (bounded)
-        // before the tensor memory and the shared memory are given up
-        if (fail_bar >= 0) {
-            atomicExch(err, kTmaErrTimeout);
-            mbar_wait(fail_bar < 2 ? &bar_ld[fail_bar] : &bar_mma[fail_bar - 2], fail_par);
-        }
-        tc_fence_before_sync();
-        __syncthreads();
-        if (warp == 0) tc_dealloc(tbase, 256);
-        return;
-    }
-    if (nch == 0)
-        for (int g = 0; g < ngrp; g++) epilogue(g, true);
     tc_fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc_dealloc(tbase, 256);
+    if (warp == 0) tc_dealloc(tbase, kTmemCols);
 }
 
 }  // namespace
@@ -416,21 +496,40 @@ int tc_build(SpmeEngine *e)
     return kOk;
 }
 
-size_t spread_tc_smem(int K)
+// Dynamic shared memory of k_spread_tc<K, nrhs>: the copy ring and two force
+// operand buffers.
+static size_t spread_tc_smem(int K, int nrhs)
 {
-    return 2 * (size_t)(2 * K * kTcChunk + 2 * kTcCols * kTcChunk + kTcChunk * kTcRows + kTcRhs * 3 * kTcChunk) *
-           sizeof(float);
+    const size_t ncol = (size_t)nrhs * 3 * kTcRows;
+    return ((size_t)kTcRing * (2 * K * kTcChunk + kTcChunk * kTcRows) + 4 * ncol * kTcChunk) * sizeof(float);
+}
+
+template <int NRHS>
+static int spread_tc_launch_n(SpmeEngine *e, int nr, int r0, int nsm, cudaStream_t s)
+{
+    const size_t sm = spread_tc_smem(256, NRHS);
+    SDT_CUDA(cudaFuncSetAttribute(k_spread_tc<256, NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int nby = 256 / kTcBY, nblk = nby * (256 / kTcBZ);
+    k_spread_tc<256, NRHS><<<std::min(nsm, nblk), kTcThreads, sm, s>>>(e->npos, nby, nblk, e->d_tc_start,
+                                                                        e->d_tc_slot, e->d_tc_w, e->d_tc_bx,
+                                                                        e->d_fs_sp, e->XS, e->d_cgrid, r0, nr,
+                                                                        e->d_err);
+    SDT_LAUNCH_CHECK();
+    return kOk;
 }
 
 int spread_tc_launch(SpmeEngine *e, int nr, int r0, cudaStream_t s)
 {
     if (e->K != 256) return set_error(e, kErrUnsupported, "tensor-core spread needs K = 256");
-    const size_t sm = spread_tc_smem(256);
-    SDT_CUDA(cudaFuncSetAttribute(k_spread_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_spread_tc<256><<<dim3(256 / kTcBY, 256 / kTcBZ), kTcThreads, sm, s>>>(
-        e->npos, 256 / kTcBY, e->d_tc_start, e->d_tc_slot, e->d_tc_w, e->d_tc_bx, e->d_fs_sp, e->XS, e->d_cgrid,
-        r0, nr, e->d_err);
-    SDT_LAUNCH_CHECK();
+    int nsm = 0;
+    SDT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+    // up to 16 RHS per launch, all in one accumulator (N = 96 for <= 8)
+    for (int g0 = 0; g0 < nr; g0 += 16) {
+        const int gn = std::min(16, nr - g0);
+        const int st = gn > 8 ? spread_tc_launch_n<16>(e, gn, r0 + g0, nsm, s)
+                              : spread_tc_launch_n<8>(e, gn, r0 + g0, nsm, s);
+        if (st != kOk) return st;
+    }
     return kOk;
 }
 

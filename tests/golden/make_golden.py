@@ -172,6 +172,49 @@ def bd_cfg3_case(name, nsteps=10, tol=None, max_iters=None):
                         nsteps=np.array(nsteps), tol=np.array(tol))
 
 
+# Dense-Ewald trajectory: a small suspension on the reference driver's
+# default mobility (mob-method ewald) with Lanczos, 4 RHS per interval; 3N is
+# a multiple of 8 (the reference's PadLen), so the random block needs no
+# padding.
+BD_EWALD = dict(npos=304, phi=0.2, seed_pos=17, seed_z=31, dt=1e-3, interval=4, nsteps=8, ewald_tol=1e-4,
+                lanczos_tol=1e-8, max_iters=100, steric_r0=2.0, steric_k0=125.0)
+
+
+def bd_ewald_case(name):
+    """First BD_EWALD["nsteps"] steps of BDSimBox::Advance
+    (src/simbox/simbox_bd.cc:296-366) with the reference's MobEwald
+    (ewald-tol 1e-4, default xi), BrwnLanczos (4 RHS every 4 steps, tol
+    1e-8) and StericForce, FP64, driven by the device integrator's random
+    vectors (numpy restatement of its Philox4x32-10 + Box-Muller draw).
+    Stores pos(k) - pos(0) after every step."""
+    from stokesdt_b200 import workloads as wl
+    c = BD_EWALD
+    N, n3 = c["npos"], 3 * c["npos"]
+    L = wl.box_for(N, c["phi"])
+    rdi = np.ones(N)
+    pos0 = wl.rsa_positions(N, L, c["seed_pos"]).reshape(-1)
+    ew = ref.RefMob.ewald(rdi, L, tol=c["ewald_tol"])
+    lz = ref.RefLanczos(n3, c["max_iters"], c["interval"], c["lanczos_tol"])
+    st = ref.RefSteric(rdi, L, c["steric_r0"], c["steric_k0"])
+    pos = pos0.copy()
+    disp_all, iters = [], []
+    y = None
+    for k in range(c["nsteps"]):
+        irhs = k % c["interval"]
+        if irhs == 0:
+            z = so.bd_gaussian(c["seed_z"], k, c["interval"], n3)
+            ew.update(pos, rdi)
+            y, its = lz.compute(ew, z)
+            iters.append(its[0])
+        f = st.accumulate(np.mod(pos, L), np.zeros(n3))
+        disp = ew.mulvec(f[None, :], c["dt"], np.sqrt(2.0 * c["dt"]), y[irhs][None, :])[0, :n3]
+        pos = pos + disp
+        disp_all.append(pos - pos0)
+        print(f"{name}: step {k + 1}, |pos - pos0| {np.linalg.norm(pos - pos0):.6f}")
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), d=np.array(disp_all), iters=np.array(iters),
+                        box=np.array(L), **{k: np.array(v) for k, v in c.items()})
+
+
 CFG2_PROJ_SEED, CFG2_NPROJ = 2024, 64
 
 
@@ -287,7 +330,11 @@ def main():
     ap.add_argument("--bd", action="store_true", help="only the config-3 trajectory fixture")
     ap.add_argument("--bd-tight", action="store_true",
                     help="only the config-3 trajectory fixture at Lanczos tol 1e-8")
+    ap.add_argument("--bd-ewald", action="store_true", help="only the dense-Ewald trajectory fixture")
     a = ap.parse_args()
+    if a.bd_ewald:
+        bd_ewald_case("bd_ewald_traj")
+        return
     if a.bd:
         bd_cfg3_case("bd_cfg3_traj")
         return

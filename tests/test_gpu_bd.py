@@ -148,3 +148,33 @@ def _config3_vs_reference(name, tol, max_iters, bar):
         assert abs(np.linalg.norm(d) / g["norms"][k] - 1.0) < bar, k
     assert worst < bar, worst
     assert bd.info()["not_converged"] == 0
+
+
+def test_dense_ewald_trajectory_vs_reference(gpu_available):
+    """The integrator on the dense Ewald mobility (the reference driver's
+    default mob-method): N=304, phi=0.2, ewald-tol 1e-4, 4 RHS per interval,
+    Lanczos tol 1e-8, steric r0=2 k0=125, 8 steps, against the FP64
+    trajectory the reference's own MobEwald, BrwnLanczos and StericForce
+    produce from the same random vectors (tests/golden/bd_ewald_traj.npz).
+    Everything is FP64 and the Lanczos iterates are converged far below the
+    bar: 1e-6 relative on pos(k) - pos(0) per step."""
+    import stokesdt_b200 as sdt
+    from stokesdt_b200 import workloads as wl
+    from conftest import golden
+    g = golden("bd_ewald_traj")
+    N, L = int(g["npos"]), float(g["box"])
+    n3 = 3 * N
+    pos0 = wl.rsa_positions(N, L, int(g["seed_pos"])).reshape(-1)
+    m = sdt.MobEwald(N, np.ones(N), L, float(g["ewald_tol"]))
+    assert m.Init(), m.last_error
+    lz = sdt.BrwnLanczos(n3, int(g["max_iters"]), int(g["interval"]), float(g["lanczos_tol"]), reorth=True)
+    assert lz.Init()
+    st = sdt.StericForce(N, np.ones(N), L, float(g["steric_r0"]), float(g["steric_k0"]))
+    assert st.Init()
+    bd = sdt.BDIntegrator(m, lz, st, dt=float(g["dt"]), mob_interval=int(g["interval"]), seed=int(g["seed_z"]))
+    bd.set_positions(pos0)
+    for k in range(int(g["nsteps"])):
+        bd.Advance(1)
+        d = bd.get_positions() - pos0
+        assert rel_err(g["d"][k], d) < 1e-6, k
+    assert bd.info()["not_converged"] == 0

@@ -79,3 +79,43 @@ def test_bdrun_config3_first_steps_vs_reference_trajectory(gpu_available, tmp_pa
         pk = P @ d
         assert np.linalg.norm(pk - g["proj"][k]) / np.linalg.norm(g["proj"][k]) < 1e-4, k
         assert abs(np.linalg.norm(d) / g["norms"][k] - 1.0) < 1e-4, k
+
+
+def test_bdrun_dense_ewald_vs_reference_trajectory(gpu_available, tmp_path):
+    """bdrun with `mob-method ewald` (the reference driver's default
+    mobility, src/simbox/simbox_bd.cc:93-103; ewald-tol 1e-4) and Lanczos
+    (4 RHS per interval, tol 1e-8) on N=304: its frames for steps 1..8
+    against the FP64 trajectory of the reference's own MobEwald, BrwnLanczos
+    and StericForce from the same random vectors
+    (tests/golden/bd_ewald_traj.npz): 1e-6 relative per step."""
+    import stokesdt_b200 as sdt
+    from stokesdt_b200 import workloads as wl
+    from conftest import golden
+    g = golden("bd_ewald_traj")
+    N, L = int(g["npos"]), float(g["box"])
+    n3 = 3 * N
+    nsteps = int(g["nsteps"])
+    pos0 = wl.rsa_positions(N, L, int(g["seed_pos"]))
+    sdt.write_xyz(tmp_path / "start.xyz", pos0, L)
+    (tmp_path / "run.cfg").write_text(
+        f"delta-t {float(g['dt'])!r}\nmob-method ewald\newald-tol {float(g['ewald_tol'])!r}\n"
+        f"brownian-method lanczos\nmob-interval {int(g['interval'])}\nlanczos-maxiters {int(g['max_iters'])}\n"
+        f"lanczos-maxnrhs {int(g['interval'])}\nlanczos-tol {float(g['lanczos_tol'])!r}\n"
+        f"traj-startstep 0\ntraj-interval 1\ntraj-output {tmp_path / 'traj.xyz'}\nrandom-seed {int(g['seed_z'])}\n")
+    (tmp_path / "run.mod").write_text(f"par N 1.0 0.0\nsteric {float(g['steric_r0'])} {float(g['steric_k0'])}\n")
+    exe = os.path.join(ROOT, "stokesdt_b200", "bdrun")
+    res = subprocess.run([exe, "--config", str(tmp_path / "run.cfg"), "--model", str(tmp_path / "run.mod"),
+                          "--xyz", str(tmp_path / "start.xyz"), "-n", str(nsteps)], capture_output=True,
+                         text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "dense Ewald" in res.stdout
+    start = sdt.read_xyz(tmp_path / "start.xyz")[0].reshape(-1)
+    lines = (tmp_path / "traj.xyz").read_text().splitlines()
+    assert len(lines) == nsteps * (N + 2)
+    for k in range(nsteps):
+        frame = lines[k * (N + 2):(k + 1) * (N + 2)]
+        assert int(frame[1].split()[0]) == k + 1
+        pos = np.array([[float(v) for v in l.split()[1:4]] for l in frame[2:]]).reshape(-1)
+        d = pos - start
+        assert np.linalg.norm(d - g["d"][k]) / np.linalg.norm(g["d"][k]) < 1e-6, k
+    assert n3 == g["d"].shape[1]

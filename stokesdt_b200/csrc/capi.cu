@@ -431,7 +431,8 @@ int sdt_bd_get_positions(sdt_bd *h, double *pos)
         b->last_error = "copying positions from the device failed";
         return SDT_ERR_CUDA;
     }
-    return sdt::spme_check_device_error(h->s.mob);
+    // the dense Ewald kernels have no device error word (no bounded waits)
+    return h->s.mob ? sdt::spme_check_device_error(h->s.mob) : SDT_OK;
 }
 
 int sdt_bd_set_step(sdt_bd *h, long long istep)
@@ -506,7 +507,8 @@ int sdt_bd_synchronize(sdt_bd *h)
         h->s.last_error = "synchronize failed";
         return SDT_ERR_CUDA;
     }
-    return sdt::spme_check_device_error(h->s.mob);
+    // the dense Ewald kernels have no device error word (no bounded waits)
+    return h->s.mob ? sdt::spme_check_device_error(h->s.mob) : SDT_OK;
 }
 
 const char *sdt_bd_last_error(const sdt_bd *h) { return h ? h->s.last_error.c_str() : ""; }

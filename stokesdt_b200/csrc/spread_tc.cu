@@ -198,11 +198,11 @@ k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const in
             mbar_init(&ring_empty[i], 1);
         }
         for (int i = 0; i < 2; i++) {
-            mbar_init(&op_full[i], kTcBuilders);
+            mbar_init(&op_full[i], kTcBuildWarps);  // one arrive per builder warp
             mbar_init(&op_empty[i], 1);
         }
         mbar_init(&acc_full, 1);
-        mbar_init(&acc_empty, kTcBuilders);
+        mbar_init(&acc_empty, kTcBuildWarps);
         abort_flag = 0;
         fence_barrier_init();
     }
@@ -300,22 +300,39 @@ k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const in
         const int bt = tid - 64;
         const int q4 = warp & 3;                         // tensor-memory lane quarter of this warp
         const int half = (warp - 2) >> 2;                // which half of the column groups it writes
-        // forces gathered for (component column cc, entry k) = (idx / 16, idx % 16), idx = bt + u * 256
-        auto gather = [&](int qc, float (&f)[FPT]) {
+        // forces for (component column cc, entry k) = (idx / 16, idx % 16),
+        // idx = bt + u * 256, in two stages a chunk apart so no load waits
+        // on another inside a chunk: the entries' particle slots two chunks
+        // ahead, their forces one chunk ahead
+        // per-thread constants: entry k of each force, the force row in
+        // fs_sp (null for columns past nr or past NF) and the operand offset
+        // of its row 0 (rows 1..3 follow at +4 floats: columns 4 cc .. 4 cc
+        // + 3 share one 8-row core-matrix group)
+        int fk[FPT];
+        const float *frow[FPT];
+        uint32_t foff[FPT];
 #pragma unroll
-            for (int u = 0; u < FPT; u++) {
-                const int idx = bt + u * kTcBuilders;
-                f[u] = 0.0f;
-                if (idx < NF) {
-                    const int cc = idx / kTcChunk, k = idx % kTcChunk, rl = cc / 3;
-                    const int s = tc_slot[qc + k];
-                    if (rl < nr && s >= 0) f[u] = fs_sp[(size_t)(3 * (r0 + rl) + cc % 3) * n + s];
-                }
-            }
+        for (int u = 0; u < FPT; u++) {
+            const int idx = bt + u * kTcBuilders, cc = idx / kTcChunk;
+            fk[u] = idx % kTcChunk;
+            frow[u] = (idx < NF && cc / 3 < nr) ? fs_sp + (size_t)(3 * r0 + cc) * n : nullptr;
+            foff[u] = idx < NF ? tc_kmajor_offset(cc * kTcRows, fk[u], kTcChunk) / 4 : 0u;
+        }
+        static_assert(kTcRows == 4, "a column's 4 rows are one 16-byte group of row weights");
+        auto load_slots = [&](int qc, int (&sl)[FPT]) {
+#pragma unroll
+            for (int u = 0; u < FPT; u++) sl[u] = (qc >= 0 && frow[u]) ? tc_slot[qc + fk[u]] : -1;
         };
+        auto load_forces = [&](const int (&sl)[FPT], float (&f)[FPT]) {
+#pragma unroll
+            for (int u = 0; u < FPT; u++) f[u] = sl[u] >= 0 ? frow[u][sl[u]] : 0.0f;
+        };
+        const size_t kkx = (size_t)K * K * XS;  // one (RHS, component) grid
         auto epilogue = [&](int b, bool zero) {
             const int by = b % nby, bz = b / nby;
             const int kx = q4 * 32 + lane;
+            // row (z, y) = (2 bz + row / 2, 2 by + row % 2) of component grid 3 r0 + cc
+            float2 *const base = cgrid + (size_t)3 * r0 * kkx + ((size_t)kTcBZ * bz * K + kTcBY * by) * XS + kx;
             const uint32_t trow = tbase + ((uint32_t)(q4 * 32) << 16);
             constexpr int NG = NCOL / 16;
 #pragma unroll 1
@@ -331,43 +348,40 @@ k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const in
                 }
 #pragma unroll
                 for (int jj = 0; jj < 16; jj++) {
-                    const int col = gg * 16 + jj;
-                    const int cc = col / kTcRows, row = col % kTcRows, rl = cc / 3;
-                    const int z = kTcBZ * bz + row / kTcBY, y = kTcBY * by + row % kTcBY;
-                    float2 *gp = cgrid + (((size_t)(3 * (r0 + rl) + cc % 3) * K + z) * K + y) * XS;
-                    if (rl < nr) {
-                        gp[kx] = make_float2(re[jj], kx == 0 ? 0.0f : im[jj]);
+                    const int cc = gg * (16 / kTcRows) + jj / kTcRows, row = jj % kTcRows;
+                    float2 *gp = base + (size_t)cc * kkx + ((size_t)(row / kTcBY) * K + row % kTcBY) * XS;
+                    if (cc / 3 < nr) {
+                        gp[0] = make_float2(re[jj], kx == 0 ? 0.0f : im[jj]);
                         if (kx == 0) gp[H] = make_float2(im[jj], 0.0f);
                     }
                 }
             }
         };
-        float fcur[FPT], fnext[FPT];
-        // next chunk of the walk after (b, c): the same block's next chunk or
-        // the first chunk of the next non-empty block; false at the end
-        auto next_chunk = [&](int b, int c, int nch, int q0, int &qn) {
-            if (c + 1 < nch) {
-                qn = q0 + (c + 1) * kTcChunk;
-                return true;
-            }
-            for (int b2 = b + (int)gridDim.x; b2 < nblk; b2 += gridDim.x) {
-                int q2;
-                if (chunks(b2, q2) > 0) {
-                    qn = q2;
-                    return true;
-                }
-            }
-            return false;
+        // lookahead cursor over the walk's chunks (empty blocks skipped);
+        // q = -1 past the end
+        struct Cursor {
+            int b, q0, nch, c;
         };
-        int first_q = -1;
-        for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
-            int q0;
-            if (chunks(b, q0) > 0) {
-                first_q = q0;
-                break;
+        auto advance = [&](Cursor &u) {
+            if (u.b >= nblk) return;
+            u.c++;
+            while (u.c >= u.nch) {
+                u.b += gridDim.x;
+                if (u.b >= nblk) return;
+                u.nch = chunks(u.b, u.q0);
+                u.c = 0;
             }
-        }
-        if (first_q >= 0) gather(first_q, fnext);
+        };
+        auto q_of = [&](const Cursor &u) { return u.b < nblk ? u.q0 + u.c * kTcChunk : -1; };
+        Cursor la{(int)blockIdx.x, 0, 0, -1};
+        if (la.b < nblk) la.nch = chunks(la.b, la.q0);
+        advance(la);  // step 0
+        int snext[FPT];
+        float fcur[FPT], fnext[FPT];
+        load_slots(q_of(la), snext);
+        load_forces(snext, fnext);  // step 0 (waits once, before the first chunk)
+        advance(la);                // step 1
+        load_slots(q_of(la), snext);
         int step = 0, j = 0;
         bool ok = true;
         for (int b = blockIdx.x; b < nblk && ok; b += gridDim.x) {
@@ -380,10 +394,15 @@ k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const in
             for (int c = 0; c < nch; c++, step++) {
 #pragma unroll
                 for (int u = 0; u < FPT; u++) fcur[u] = fnext[u];
-                int qn;
-                if (next_chunk(b, c, nch, q0, qn)) gather(qn, fnext);
+                load_forces(snext, fnext);  // step + 1 (slots loaded a chunk ago)
+                advance(la);                // step + 2
+                load_slots(q_of(la), snext);
                 const int s = step % kTcRing, u = step / kTcRing, ob = step & 1, v = step >> 1;
-                if (!tc_wait(&ring_full[s], u & 1, abort) || !tc_wait(&op_empty[ob], (v & 1) ^ 1, abort)) {
+                // every lane waits; the warp leaves together (its arrive and
+                // tensor-memory loads are warp-wide)
+                bool w_ok = tc_wait(&ring_full[s], u & 1, abort);
+                if (w_ok) w_ok = tc_wait(&op_empty[ob], (v & 1) ^ 1, abort);
+                if (!__all_sync(0xffffffffu, w_ok)) {
                     ok = false;
                     break;
                 }
@@ -391,31 +410,31 @@ k_spread_tc(int n, int nby, int nblk, const int *__restrict__ tc_start, const in
                 float *bh = opb + ob * 2 * B_FL, *bl = bh + B_FL;
 #pragma unroll
                 for (int uu = 0; uu < FPT; uu++) {
-                    const int idx = bt + uu * kTcBuilders;
-                    if (idx < NF) {
-                        const int cc = idx / kTcChunk, k = idx % kTcChunk;
+                    if (bt + uu * kTcBuilders < NF) {
+                        const float4 w = *reinterpret_cast<const float4 *>(sW + fk[uu] * kTcRows);
+                        const float x[4] = {fcur[uu] * w.x, fcur[uu] * w.y, fcur[uu] * w.z, fcur[uu] * w.w};
 #pragma unroll
                         for (int row = 0; row < kTcRows; row++) {
-                            const float x = fcur[uu] * sW[k * kTcRows + row];
-                            const float hi = tf32_round(x), lo = tf32_round(x - hi);
-                            const uint32_t off = tc_kmajor_offset(cc * kTcRows + row, k, kTcChunk) / 4;
-                            bh[off] = hi;
-                            bl[off] = lo;
+                            const float hi = tf32_round(x[row]), lo = tf32_round(x[row] - hi);
+                            bh[foff[uu] + 4 * row] = hi;
+                            bl[foff[uu] + 4 * row] = lo;
                         }
                     }
                 }
                 fence_proxy_async_smem();
-                mbar_arrive(&op_full[ob]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&op_full[ob]);
             }
             if (!ok) break;
-            if (!tc_wait(&acc_full, j & 1, abort)) {
+            if (!__all_sync(0xffffffffu, tc_wait(&acc_full, j & 1, abort))) {
                 ok = false;
                 break;
             }
             tc_fence_after_sync();
             epilogue(b, false);
             tc_fence_before_sync();
-            mbar_arrive(&acc_empty);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty);
             j++;
         }
         if (!ok) atomicExch(err, kTmaErrTimeout);

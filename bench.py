@@ -17,6 +17,12 @@ buffers (H2D of pos, Z, F, Y in / D2H of Y, disp every step).
 For N > 1 (launched by torchrun) every rank runs an independent replica
 system (weak scaling, no data-path collective); the timed region is bracketed
 by barriers and the reported time is the max over ranks.
+
+At N = 1 the config-2 line also carries `other_configs`: short runs of
+config 3 (trajectory), config 4 (batched systems) and config 5 (served
+stream), each a child process started after the config-2 measurement with
+its own timing and clock record (--no-other-configs skips them; each also
+runs alone with --workload cfg3|cfg4|cfg5).
 """
 from __future__ import annotations
 
@@ -58,6 +64,8 @@ def parse_args():
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: a few mobility products, no timing output")
     ap.add_argument("--profile-rhs", type=int, default=1, help="RHS per product in --profile-case")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="config 2 at N=1: skip the short config 3/4/5 legs attached to the line")
     return ap.parse_args()
 
 
@@ -636,10 +644,45 @@ def run_b200(args):
             "stage_ms_16rhs": {k: round(v, 4) for k, v in stages.items()},
             "cufft_reference": cufft,
         }
-        print(json.dumps(out))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return out if rank == 0 else None
+
+
+# short legs of configs 3-5 run after the config-2 line's own measurement (N=1
+# only), each its own process with its own clock record: (workload, args, timeout s)
+OTHER_CONFIGS = (("cfg3", ["--steps", "20", "--warmup", "3", "--no-cpu-baseline"], 600),
+                 ("cfg4", ["--steps", "1", "--warmup", "3"], 900),
+                 ("cfg5", ["--steps", "5", "--warmup", "3"], 600))
+OTHER_KEYS = ("metric", "value", "unit", "ms_per_step", "higher_is_better", "e2e", "clocks", "gpu_launches",
+              "latency_ms", "lanes_mode_systems_per_s_rank0", "plain_per_system_systems_per_s_rank0",
+              "packed_over_plain", "phase_ms_rank0", "per_rate", "plain_per_request_path", "batching_rank0",
+              "lanczos_iters_median", "roofline")
+
+
+def run_other_configs():
+    """Run the short config 3/4/5 legs as child processes and keep the main
+    fields of their JSON lines (or the reason a leg gave none)."""
+    import subprocess
+    res = {}
+    for wk, extra, tmo in OTHER_CONFIGS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wk, "--no-other-configs"] + extra
+        t0 = time.perf_counter()
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=tmo)
+            line = [l for l in p.stdout.splitlines() if l.startswith("{")]
+            if p.returncode != 0 or not line:
+                res[wk] = {"error": f"exit {p.returncode}: {(p.stderr or '').strip()[-300:]}"}
+            else:
+                d = json.loads(line[-1])
+                res[wk] = {k: d[k] for k in OTHER_KEYS if k in d}
+                res[wk]["config"] = d.get("config", {}).get("workload")
+        except subprocess.TimeoutExpired:
+            res[wk] = {"error": f"did not finish within {tmo} s"}
+        res[wk]["wall_s"] = round(time.perf_counter() - t0, 1)
+        log(f"{wk}: {res[wk].get('value', res[wk].get('error'))}")
+    return res
 
 
 def run_b200_traj(args, w):
@@ -1151,8 +1194,19 @@ def main():
         w = wl.WORKLOADS[args.workload]
         if w.nsteps > 0:
             run_b200_traj(args, w)
-        else:
-            run_b200(args)
+            return
+        out = run_b200(args)
+        if out is None:
+            return
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if world == 1 and args.workload == "cfg2" and not args.no_other_configs and not args.profile_case:
+            # the config-2 engines are gone with run_b200; give their memory back first
+            import gc
+            import torch
+            gc.collect()
+            torch.cuda.empty_cache()
+            out["other_configs"] = run_other_configs()
+        print(json.dumps(out))
 
 
 if __name__ == "__main__":

@@ -365,6 +365,9 @@ __device__ __forceinline__ void pair_apply_block(int n, const long long *__restr
     static_assert(RB >= 1 && RB <= 32 && (32 % RB) == 0, "RB must divide the warp");
     constexpr int kPairsPerStep = 32 / RB;
     constexpr int kFB = RB < 8 ? RB : 8;  // force loads in flight per lane
+    // 32-pair batches of the list in flight per warp: with one RHS a pair
+    // carries little work, so the stream needs more loads in flight
+    constexpr int PF = RB == 1 ? 4 : 1;
     __shared__ float4 se[kRsWarps][32];
     __shared__ float2 sc[kRsWarps][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -376,23 +379,32 @@ __device__ __forceinline__ void pair_apply_block(int n, const long long *__restr
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
     // slots past the row end hold a zero block on a valid source (s itself)
     const float2 pad = make_float2(0.0f, __int_as_float(s));
-    float4 ne = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float2 nc = pad;
-    if (b + lane < e) {
-        ne = __ldcs(&pl_e[b + lane]);
-        nc = __ldcs(&pl_c[b + lane]);
+    float4 ne[PF];
+    float2 nc[PF];
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+        ne[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        nc[u] = pad;
+        if (b + 32 * u + lane < e) {
+            ne[u] = __ldcs(&pl_e[b + 32 * u + lane]);
+            nc[u] = __ldcs(&pl_c[b + 32 * u + lane]);
+        }
     }
-    for (long long base = b; base < e; base += 32) {
+    for (long long base0 = b; base0 < e; base0 += 32 * PF)
+#pragma unroll
+    for (int ub = 0; ub < PF; ub++) {
+        const long long base = base0 + 32 * ub;
+        if (base >= e) break;  // the same in every lane
         __syncwarp();
-        se[warp][lane] = ne;
-        sc[warp][lane] = nc;
+        se[warp][lane] = ne[ub];
+        sc[warp][lane] = nc[ub];
         __syncwarp();
-        const long long qn = base + 32 + lane;
-        ne = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        nc = pad;
+        const long long qn = base + 32 * PF + lane;
+        ne[ub] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        nc[ub] = pad;
         if (qn < e) {
-            ne = __ldcs(&pl_e[qn]);
-            nc = __ldcs(&pl_c[qn]);
+            ne[ub] = __ldcs(&pl_e[qn]);
+            nc[ub] = __ldcs(&pl_c[qn]);
         }
         const int cnt = (int)min(32LL, e - base);
         const int steps = (cnt + kPairsPerStep - 1) / kPairsPerStep;

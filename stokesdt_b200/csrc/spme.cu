@@ -275,7 +275,7 @@ __global__ void k_seg_fill(int n, int p, int K, int nby, const int *__restrict__
 // consecutive slots s, so the writes are coalesced.
 __global__ void k_gather_forces(int n, int nr, const double *__restrict__ f, int ldf,
                                 const int *__restrict__ sp_perm, const double *__restrict__ scale,
-                                float *__restrict__ fs_sp)
+                                float *__restrict__ fs_sp, float *__restrict__ zero)
 {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (idx >= (long long)n * nr) return;
@@ -285,6 +285,9 @@ __global__ void k_gather_forces(int n, int nr, const double *__restrict__ f, int
     const double sc = scale ? scale[i] : 1.0;
     const double *fi = f + (size_t)r * ldf + 3 * i;
     for (int c = 0; c < 3; c++) fs_sp[((size_t)r * 3 + c) * n + s] = (float)(fi[c] * sc);
+    // optionally clear the [nr][3n] array the interpolation accumulates into
+    if (zero)
+        for (int c = 0; c < 3; c++) zero[(size_t)r * 3 * n + 3 * s + c] = 0.0f;
 }
 
 // FP64 caller forces -> FP32 copy in cell order, [s][r][4] (fourth float
@@ -1647,11 +1650,11 @@ int spme_mulvec(SpmeEngine *e, int mode, int nrhs, double alpha, int ldf, const 
         const int nr = std::min(chunk, nrhs - r0);
         const double *f = d_f + (size_t)r0 * ldf;
         double *v = d_v + (size_t)r0 * ldv;
-        SDT_CUDA(cudaMemsetAsync(e->d_vrecip, 0, (size_t)nr * n3 * sizeof(float), e->stream));
-        SDT_CUDA(cudaMemsetAsync(e->d_vreal, 0, (size_t)nr * n3 * sizeof(float), e->stream));
+        // vrecip (interpolation atomics) is cleared by the first force gather;
+        // vreal needs no clearing: the real-space kernels store every row
         if (mode != 1) {
             k_gather_forces<<<grid1d((long long)n * nr, 256), 256, 0, e->stream>>>(
-                n, nr, f, ldf, e->d_sp_perm, nullptr, e->d_fs_sp);
+                n, nr, f, ldf, e->d_sp_perm, nullptr, e->d_fs_sp, e->d_vrecip);
             SDT_LAUNCH_CHECK();
         }
         if (mode != 2) {
@@ -1708,12 +1711,12 @@ int spme_mulvec(SpmeEngine *e, int mode, int nrhs, double alpha, int ldf, const 
                 st = recip_dispatch(e, nr, e->d_tab0, nullptr);
                 if (st != kOk) return st;
                 k_gather_forces<<<grid1d((long long)n * nr, 256), 256, 0, e->stream>>>(
-                    n, nr, f, ldf, e->d_sp_perm, e->d_rdi2, e->d_fs_sp);
+                    n, nr, f, ldf, e->d_sp_perm, e->d_rdi2, e->d_fs_sp, nullptr);
                 SDT_LAUNCH_CHECK();
                 st = recip_dispatch(e, nr, e->d_tab2, nullptr);
                 if (st != kOk) return st;
                 k_gather_forces<<<grid1d((long long)n * nr, 256), 256, 0, e->stream>>>(
-                    n, nr, f, ldf, e->d_sp_perm, nullptr, e->d_fs_sp);
+                    n, nr, f, ldf, e->d_sp_perm, nullptr, e->d_fs_sp, nullptr);
                 SDT_LAUNCH_CHECK();
                 st = recip_dispatch(e, nr, e->d_tab2, e->d_rdi2);
                 if (st != kOk) return st;
@@ -1742,7 +1745,7 @@ int spme_spectrum(SpmeEngine *e, int nrhs, int ldf, const double *d_f, float *d_
     int st = spme_reserve(e, nrhs);
     if (st != kOk) return st;
     k_gather_forces<<<grid1d((long long)n * nrhs, 256), 256, 0, e->stream>>>(n, nrhs, d_f, ldf, e->d_sp_perm,
-                                                                           nullptr, e->d_fs_sp);
+                                                                           nullptr, e->d_fs_sp, nullptr);
     SDT_LAUNCH_CHECK();
     st = recip_dispatch(e, nrhs, e->d_tab0, nullptr, 0, nullptr, true);
     if (st != kOk) return st;

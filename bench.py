@@ -137,7 +137,7 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 # kernel behind each profiled stage of a 16-RHS product (K = 256: the
 # tensor-core spread takes calls of >= 8 RHS)
-STAGE_KERNEL = {"gather_forces": "k_gather_forces + k_gather_forces_rs", "real_space": "k_pair_apply<16>",
+STAGE_KERNEL = {"gather_forces": "k_gather_both", "real_space": "k_pair_apply<16>",
                 "spread_tc": "k_spread_tc<K,16>", "spread_xfwd": "k_spread_xfwd<K>",
                 "yfft_fwd": "k_ypass_tma<K,fwd>", "zfft_influence": "k_zpass_fused_tma<K>",
                 "yfft_inv": "k_ypass_tma<K,inv>", "xinv_interp": "k_xinv_interp<K>", "combine": "k_combine"}

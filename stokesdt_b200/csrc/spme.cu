@@ -290,13 +290,30 @@ __global__ void k_gather_forces(int n, int nr, const double *__restrict__ f, int
         for (int c = 0; c < 3; c++) zero[(size_t)r * 3 * n + 3 * s + c] = 0.0f;
 }
 
-// FP64 caller forces -> FP32 copy in cell order, [s][r][4] (fourth float
-// zero): one thread per particle i (coalesced reads of f), writing its nr
-// float4 values contiguously at slot rs_inv[i].
-__global__ void k_gather_forces_rs(int n, int nr, const double *__restrict__ f, int ldf,
-                                   const int *__restrict__ rs_inv, float4 *__restrict__ fs_rs)
+// Both force copies of a product in one launch.  Blocks [0, nb_sp) do
+// k_gather_forces' work and clear the interpolation accumulator `zero`; the
+// blocks after them make the FP32 copy in cell order, [s][r][4] (fourth
+// float zero): one thread per particle i (coalesced reads of f), writing its
+// nr float4 values contiguously at slot rs_inv[i].  A product that needs
+// only one copy launches only its blocks.
+__global__ void k_gather_both(int n, int nr, const double *__restrict__ f, int ldf,
+                              const int *__restrict__ sp_perm, float *__restrict__ fs_sp,
+                              float *__restrict__ zero, int nb_sp, const int *__restrict__ rs_inv,
+                              float4 *__restrict__ fs_rs)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((int)blockIdx.x < nb_sp) {
+        const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        if (idx >= (long long)n * nr) return;
+        const int s = (int)(idx % n);
+        const int r = (int)(idx / n);
+        const double *fi = f + (size_t)r * ldf + 3 * sp_perm[s];
+        for (int c = 0; c < 3; c++) {
+            fs_sp[((size_t)r * 3 + c) * n + s] = (float)fi[c];
+            zero[(size_t)r * 3 * n + 3 * s + c] = 0.0f;
+        }
+        return;
+    }
+    const int i = (blockIdx.x - nb_sp) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 *out = fs_rs + (size_t)rs_inv[i] * nr;
     for (int r = 0; r < nr; r++) {
@@ -1652,14 +1669,12 @@ int spme_mulvec(SpmeEngine *e, int mode, int nrhs, double alpha, int ldf, const 
         double *v = d_v + (size_t)r0 * ldv;
         // vrecip (interpolation atomics) is cleared by the first force gather;
         // vreal needs no clearing: the real-space kernels store every row
-        if (mode != 1) {
-            k_gather_forces<<<grid1d((long long)n * nr, 256), 256, 0, e->stream>>>(
-                n, nr, f, ldf, e->d_sp_perm, nullptr, e->d_fs_sp, e->d_vrecip);
-            SDT_LAUNCH_CHECK();
-        }
-        if (mode != 2) {
-            k_gather_forces_rs<<<grid1d(n, 256), 256, 0, e->stream>>>(n, nr, f, ldf, e->d_rs_inv,
-                                                                   reinterpret_cast<float4 *>(e->d_fs_rs));
+        {
+            const int nb_sp = mode != 1 ? grid1d((long long)n * nr, 256) : 0;
+            const int nb_rs = mode != 2 ? grid1d(n, 256) : 0;
+            k_gather_both<<<nb_sp + nb_rs, 256, 0, e->stream>>>(n, nr, f, ldf, e->d_sp_perm, e->d_fs_sp,
+                                                               e->d_vrecip, nb_sp, e->d_rs_inv,
+                                                               reinterpret_cast<float4 *>(e->d_fs_rs));
             SDT_LAUNCH_CHECK();
         }
         prof_mark(e, kStGather);

@@ -13,6 +13,8 @@
 // is formed on the device every iteration exactly as the reference does
 // (brwn_lanczos.cc:181-196).  The QR of the reference (dgeqrf/dorgqr) and the
 // Cholesky QR used here differ only by column signs, which leave Y unchanged.
+// A block of one vector (k = 1) runs the same recurrence on dot-product and
+// axpy kernels, four launches per iteration (k_vec_*).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -464,6 +466,220 @@ __global__ void k_sqnorm_partial(int n, int mb, const double *__restrict__ X, in
 }
 
 // ---------------------------------------------------------------------------
+// Single-vector iteration (k = 1).  With one RHS every Gram matrix is a dot
+// product, every block product an axpy and the Cholesky QR a normalisation
+// (one pass: the second pass of a one-column Cholesky QR divides by
+// 1 + O(eps)), so an iteration's work after the mobility product takes four
+// launches over row chunks of `rows` (<= kVecMaxRows, one CTA each) instead
+// of the block path's eleven:
+//   k_vec_dot          A_i = V_i . W
+//   k_vec_axpy_dots    W -= A_i V_i ; c = V_{0..i}^T W      (reorthogonalised)
+//   k_vec_axpy_norm    W -= A_i V_i ; g = W . W             (without)
+//   k_vec_sub_norm     W -= V_{0..i} c ; g = W . W
+//   k_vec_scale        V_{i+1} = W / sqrt(g) ; next W = B_i V_i
+// Cross-CTA sums: every CTA writes its partial sums and the last CTA to
+// arrive adds them in CTA order, so the results do not depend on scheduling.
+constexpr int kVecThreads = 256;
+constexpr int kVecMaxRows = 2048;
+
+// Sum of v over the CTA, valid in thread 0; `red` holds 8 doubles and is
+// free again once every thread has returned.
+__device__ __forceinline__ double vec_cta_sum(double v, double *red)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int w = 0; w < kVecThreads / 32; w++) t += red[w];
+    return t;
+}
+
+// True in every thread of the last CTA to arrive (all CTAs' partial sums
+// are visible to it then).  That CTA resets the counter when it is done.
+__device__ __forceinline__ bool vec_last_cta(unsigned *arrive)
+{
+    __shared__ unsigned last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1 ? 1u : 0u;
+    __syncthreads();
+    if (last) __threadfence();
+    return last != 0;
+}
+
+// out[j] = sum over CTAs q of part[q * ncol + j] (lanes take q mod 32, then
+// a fixed shuffle tree; lane 0's sum is stored).
+__device__ __forceinline__ void vec_fold(int ncol, const double *part, double *out)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = w; j < ncol; j += kVecThreads / 32) {
+        double s = 0.0;
+        for (int q = lane; q < (int)gridDim.x; q += 32) s += __ldcg(&part[(size_t)q * ncol + j]);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[j] = s;
+    }
+}
+
+// The last CTA's normalisation factor from g = ||W||^2: B = sqrt(g) and
+// 1/B; a g that is not positive is a breakdown (flag 1, and 1/B = 0 so the
+// vector becomes zero and stays finite), as in chol_qr_step_warp.
+__device__ __forceinline__ void vec_norm_fold(const double *part, double *B, double *ri, double *flag)
+{
+    double d = 0.0;
+    vec_fold(1, part, &d);  // the sum lands in thread 0
+    if (threadIdx.x != 0) return;
+    if (!(d > 0.0)) {
+        *ri = 0.0;
+        *B = 0.0;
+        *flag = 1.0;
+    } else {
+        const double r = sqrt(d);
+        *B = r;
+        *ri = 1.0 / r;
+        *flag = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+k_vec_dot(int n, int rows, const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ part,
+          unsigned *__restrict__ arrive, double *__restrict__ out)
+{
+    __shared__ double red[kVecThreads / 32];
+    const int e0 = blockIdx.x * rows, e1 = min(n, e0 + rows);
+    double s = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += kVecThreads) s = fma(x[e], y[e], s);
+    s = vec_cta_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (!vec_last_cta(arrive)) return;
+    vec_fold(1, part, out);
+    if (threadIdx.x == 0) *arrive = 0u;
+}
+
+// W -= a V_i (a = *pa, V_i = V + (ma - 1) ldv); c[j] = V_j . W for j < ma.
+// The CTA keeps its chunk of the new W in shared memory; warp w takes the
+// columns 4w..4w+3, 4w+32.. (four at a time, lanes over the rows).
+__global__ void __launch_bounds__(kVecThreads)
+k_vec_axpy_dots(int n, int rows, int ma, const double *__restrict__ V, int ldv, const double *__restrict__ pa,
+                double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
+                double *__restrict__ c)
+{
+    __shared__ double sw[kVecMaxRows];
+    const int e0 = blockIdx.x * rows, len = min(n, e0 + rows) - e0;
+    const double a = *pa;
+    const double *Vi = V + (size_t)(ma - 1) * ldv + e0;
+    for (int r = threadIdx.x; r < len; r += kVecThreads) {
+        const double w = fma(-a, Vi[r], W[e0 + r]);
+        W[e0 + r] = w;
+        sw[r] = w;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    for (int j0 = 4 * wp; j0 < ma; j0 += 4 * (kVecThreads / 32)) {
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        const double *Vj = V + (size_t)j0 * ldv + e0;
+        const int nq = min(4, ma - j0);
+        for (int r = lane; r < len; r += 32) {
+            const double w = sw[r];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q < nq) s[q] = fma(Vj[(size_t)q * ldv + r], w, s[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+            if (lane == 0 && q < nq) part[(size_t)blockIdx.x * ma + j0 + q] = s[q];
+        }
+    }
+    if (!vec_last_cta(arrive)) return;
+    vec_fold(ma, part, c);
+    __syncthreads();
+    if (threadIdx.x == 0) *arrive = 0u;
+}
+
+// W -= a V_i (a = *pa); B = ||W||, 1/B and the breakdown flag.
+__global__ void __launch_bounds__(kVecThreads)
+k_vec_axpy_norm(int n, int rows, const double *__restrict__ Vi, const double *__restrict__ pa,
+                double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
+                double *__restrict__ B, double *__restrict__ ri, double *__restrict__ flag)
+{
+    __shared__ double red[kVecThreads / 32];
+    const int e0 = blockIdx.x * rows, e1 = min(n, e0 + rows);
+    const double a = *pa;
+    double s = 0.0;
+    for (int e = e0 + threadIdx.x; e < e1; e += kVecThreads) {
+        const double w = fma(-a, Vi[e], W[e]);
+        W[e] = w;
+        s = fma(w, w, s);
+    }
+    s = vec_cta_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (!vec_last_cta(arrive)) return;
+    vec_norm_fold(part, B, ri, flag);
+    if (threadIdx.x == 0) *arrive = 0u;
+}
+
+// W -= sum_{j < ma} V_j c[j]; B = ||W||, 1/B and the breakdown flag.  A
+// thread owns rows r, r + 256, .. of the chunk (at most 8).
+__global__ void __launch_bounds__(kVecThreads)
+k_vec_sub_norm(int n, int rows, int ma, const double *__restrict__ V, int ldv, const double *__restrict__ c,
+               double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
+               double *__restrict__ B, double *__restrict__ ri, double *__restrict__ flag)
+{
+    constexpr int R = kVecMaxRows / kVecThreads;
+    __shared__ double red[kVecThreads / 32];
+    const int e0 = blockIdx.x * rows, len = min(n, e0 + rows) - e0;
+    double acc[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) acc[m] = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < ma; j++) {
+        const double cj = __ldg(&c[j]);
+        const double *Vj = V + (size_t)j * ldv + e0;
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+            const int r = threadIdx.x + m * kVecThreads;
+            if (r < len) acc[m] = fma(Vj[r], cj, acc[m]);
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+        const int r = threadIdx.x + m * kVecThreads;
+        if (r < len) {
+            const double w = W[e0 + r] - acc[m];
+            W[e0 + r] = w;
+            s = fma(w, w, s);
+        }
+    }
+    s = vec_cta_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (!vec_last_cta(arrive)) return;
+    vec_norm_fold(part, B, ri, flag);
+    if (threadIdx.x == 0) *arrive = 0u;
+}
+
+// W *= *ri (the next basis vector); when Wn is given, Wn = *B Vi, the
+// V_i B_i^T term that the next iteration's product subtracts from.
+__global__ void __launch_bounds__(kVecThreads)
+k_vec_scale(int n, const double *__restrict__ ri, double *__restrict__ W, const double *__restrict__ B,
+            const double *__restrict__ Vi, double *__restrict__ Wn)
+{
+    const int e = blockIdx.x * kVecThreads + threadIdx.x;
+    if (e >= n) return;
+    W[e] *= *ri;
+    if (Wn) Wn[e] = *B * Vi[e];
+}
+
+// x *= s (host scalar)
+__global__ void __launch_bounds__(kVecThreads) k_vec_scale_host(int n, double s, double *__restrict__ x)
+{
+    const int e = blockIdx.x * kVecThreads + threadIdx.x;
+    if (e < n) x[e] *= s;
+}
+
+// ---------------------------------------------------------------------------
 
 static int gram(LanczosState *lz, int ma, const double *A, int lda, int mb, const double *B, int ldb,
                 double *d_out)
@@ -566,6 +782,14 @@ static int upload(LanczosState *lz, double *d, const double *h, size_t count)
     return kOk;
 }
 
+// Row chunk of the single-vector kernels: about one chunk per SM, a
+// multiple of 32 rows, at least 256 and at most kVecMaxRows.
+static int vec_rows(int n, int num_sms)
+{
+    const int per = (n + num_sms - 1) / std::max(1, num_sms);
+    return std::min(kVecMaxRows, std::max(kVecThreads, (per + 31) / 32 * 32));
+}
+
 // One Cholesky-QR step of one k x k Gram matrix (chol_qr_step_warp), one warp.
 __global__ void __launch_bounds__(32)
 k_chol_qr_step(int k, const double *__restrict__ G, double *__restrict__ Ri, double *__restrict__ Racc,
@@ -617,6 +841,9 @@ int lanczos_alloc(LanczosState *lz)
     lz->num_sms = dev_sms;
     LZ_CUDA(cudaFuncSetAttribute(k_gram_tall, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramSmem));
     lz->part_cap = std::max((size_t)lz->gram_chunks * 16 * 16, (size_t)64 * mmax * lz->max_nrhs);
+    // the single-vector kernels' per-chunk partial sums of up to mmax columns
+    const int vrows = vec_rows(lz->dim, lz->num_sms);
+    lz->part_cap = std::max(lz->part_cap, (size_t)((lz->dim + vrows - 1) / vrows) * mmax);
     LZ_CUDA(cudaMalloc(&lz->d_part, lz->part_cap * sizeof(double)));
     LZ_CUDA(cudaMalloc(&lz->d_arrive, sizeof(unsigned)));
     LZ_CUDA(cudaMemset(lz->d_arrive, 0, sizeof(unsigned)));
@@ -696,6 +923,43 @@ struct PhaseTimer {
     }
 };
 
+// The single-vector iteration after the product W = M V_i - B_{i-1} V_{i-1}
+// (V_i = V + it ldv, W = V_i + ldv): A_i -> dA, the optional
+// reorthogonalisation, V_{i+1} B_i = W (B_i -> dB, breakdown -> dflag) and,
+// when Wn is given, Wn = B_i V_i for the next product.
+static int vec_iteration(LanczosState *lz, int it, double *V, double *Wn, double *dA, double *dB, double *dflag,
+                         bool reorth, PhaseTimer &pt)
+{
+    const int n = lz->dim, ldv = lz->ldv;
+    const int rows = vec_rows(n, lz->num_sms), grid = (n + rows - 1) / rows;
+    double *Vi = V + (size_t)it * ldv, *W = Vi + ldv;
+    double *ri = lz->d_qr;
+    pt.begin(1);
+    k_vec_dot<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, Vi, W, lz->d_part, lz->d_arrive, dA);
+    LZ_LAUNCH();
+    if (!reorth) {
+        k_vec_axpy_norm<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, Vi, dA, W, lz->d_part, lz->d_arrive, dB,
+                                                               ri, dflag);
+        LZ_LAUNCH();
+        pt.end();
+    } else {
+        k_vec_axpy_dots<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, it + 1, V, ldv, dA, W, lz->d_part,
+                                                               lz->d_arrive, lz->d_coef);
+        LZ_LAUNCH();
+        pt.end();
+        pt.begin(2);
+        k_vec_sub_norm<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, it + 1, V, ldv, lz->d_coef, W, lz->d_part,
+                                                              lz->d_arrive, dB, ri, dflag);
+        LZ_LAUNCH();
+        pt.end();
+    }
+    pt.begin(3);
+    k_vec_scale<<<(n + kVecThreads - 1) / kVecThreads, kVecThreads, 0, lz->stream>>>(n, ri, W, dB, Vi, Wn);
+    LZ_LAUNCH();
+    pt.end();
+    return kOk;
+}
+
 static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, const double *d_z, int ldy,
                          double *d_y, int *iters_out)
 {
@@ -719,15 +983,23 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
         *iters_out = 0;
         return kOk;
     }
-    // V_0 R = Z (the spare history slot holds the breakdown flag)
-    double *init_flag = lz->d_hist + (size_t)lz->max_iters * hs;
-    st = chol_qr_device(lz, blk(0), ldv, k, true, nullptr, init_flag);
-    if (st != kOk) return st;
+    // V_0 R = Z (the spare history slot holds the breakdown flag); one
+    // vector is normalised by the norm already at hand
     std::vector<double> R(kk);
     double flag0 = 0.0;
-    st = download(lz, R.data(), lz->d_qr + kMaxBlock * kMaxBlock, (size_t)kk);
-    if (st == kOk) st = download(lz, &flag0, init_flag, 1);
-    if (st != kOk) return st;
+    if (k == 1) {
+        R[0] = normz;
+        k_vec_scale_host<<<(n + kVecThreads - 1) / kVecThreads, kVecThreads, 0, lz->stream>>>(n, 1.0 / normz,
+                                                                                              blk(0));
+        LZ_LAUNCH();
+    } else {
+        double *init_flag = lz->d_hist + (size_t)lz->max_iters * hs;
+        st = chol_qr_device(lz, blk(0), ldv, k, true, nullptr, init_flag);
+        if (st != kOk) return st;
+        st = download(lz, R.data(), lz->d_qr + kMaxBlock * kMaxBlock, (size_t)kk);
+        if (st == kOk) st = download(lz, &flag0, init_flag, 1);
+        if (st != kOk) return st;
+    }
     if (flag0 != 0.0) {
         lz->last_error = "random block is rank deficient";
         return kErrInvalid;
@@ -886,9 +1158,12 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
         double *dA = lz->d_hist + (size_t)it * hs, *dB = dA + kk, *dflag = dA + 2 * kk;
         pt.begin(0);
         if (it > 0) {
-            // W = V_{i-1} B_{i-1}^T, then W = M V_i - W
-            st = block_gemm(lz, k, blk(it - 1), ldv, Bt, k, 0.0, W, ldv);
-            if (st != kOk) break;
+            // W = V_{i-1} B_{i-1}^T (one vector: already written by the last
+            // iteration's scaling), then W = M V_i - W
+            if (k > 1) {
+                st = block_gemm(lz, k, blk(it - 1), ldv, Bt, k, 0.0, W, ldv);
+                if (st != kOk) break;
+            }
             st = mob.mulvec(k, 1.0, ldv, Vi, -1.0, ldv, W, lz->stream);
         } else {
             st = mob.mulvec(k, 1.0, ldv, Vi, 0.0, ldv, W, lz->stream);
@@ -899,27 +1174,33 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
             lz->last_error = "mobility product failed: " + mob.error();
             break;
         }
-        // A_i = V_i^T W ; W -= V_i A_i
-        pt.begin(1);
-        st = gram(lz, k, Vi, ldv, k, W, ldv, dA);
-        if (st != kOk) break;
-        st = block_gemm(lz, k, Vi, ldv, dA, k, 1.0, W, ldv, -1.0);
-        if (st != kOk) break;
-        pt.end();
-        if (reorth) {
-            pt.begin(2);
-            const int ma = (it + 1) * k;
-            st = gram(lz, ma, V, ldv, k, W, ldv, lz->d_coef);
+        if (k == 1) {
+            st = vec_iteration(lz, it, V, it + 1 < lz->max_iters ? blk(it + 2) : nullptr, dA, dB, dflag, reorth,
+                               pt);
             if (st != kOk) break;
-            st = block_gemm(lz, ma, V, ldv, lz->d_coef, k, 1.0, W, ldv, -1.0);  // W -= V C
+        } else {
+            // A_i = V_i^T W ; W -= V_i A_i
+            pt.begin(1);
+            st = gram(lz, k, Vi, ldv, k, W, ldv, dA);
+            if (st != kOk) break;
+            st = block_gemm(lz, k, Vi, ldv, dA, k, 1.0, W, ldv, -1.0);
             if (st != kOk) break;
             pt.end();
+            if (reorth) {
+                pt.begin(2);
+                const int ma = (it + 1) * k;
+                st = gram(lz, ma, V, ldv, k, W, ldv, lz->d_coef);
+                if (st != kOk) break;
+                st = block_gemm(lz, ma, V, ldv, lz->d_coef, k, 1.0, W, ldv, -1.0);  // W -= V C
+                if (st != kOk) break;
+                pt.end();
+            }
+            // W = V_{i+1} B_i; B_i^T stays on the device for the next product
+            pt.begin(3);
+            st = chol_qr_device(lz, W, ldv, k, false, dB, dflag);
+            pt.end();
+            if (st != kOk) break;
         }
-        // W = V_{i+1} B_i; B_i^T stays on the device for the next product
-        pt.begin(3);
-        st = chol_qr_device(lz, W, ldv, k, false, dB, dflag);
-        pt.end();
-        if (st != kOk) break;
         if (cudaMemcpyAsync(lz->h_hist + (size_t)it * hs, dA, (size_t)(2 * kk + 1) * sizeof(double),
                             cudaMemcpyDeviceToHost, lz->stream) != cudaSuccess ||
             cudaEventRecord(lz->ev[it], lz->stream) != cudaSuccess) {

@@ -84,6 +84,43 @@ def test_block_lanczos_vs_oracle_config1(gpu_available):
     assert rel_err(Yo.T, Y) < TOL
 
 
+@pytest.mark.parametrize("reorth", [True, False])
+def test_single_vector_vs_oracle_config1(gpu_available, reorth):
+    """One RHS (the dot-product/axpy iteration, one normalisation per step)
+    against the FP64 oracle's Lanczos on the FP64 oracle SPME, config 1, tol
+    1e-6.  With reorthogonalisation the basis stays orthonormal, so the
+    iteration count matches the oracle's to within the checks issued ahead."""
+    import stokesdt_b200 as sdt
+    from oracle import spme_oracle as so
+    g = golden("spme_cfg1")
+    N = len(g["rdi"])
+    n3 = 3 * N
+    m = sdt.MobSpme(N, g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
+    assert m.Init()
+    m.Update(g["pos"])
+    z = np.random.default_rng(9).standard_normal((1, n3))
+    lz = sdt.BrwnLanczos(n3, 100, 1, 1e-6, reorth=reorth)
+    assert lz.Init()
+    y = np.zeros((1, n3))
+    its = lz.Compute(m, 1, n3, z, n3, y)
+    assert its[0] > 0
+    assert its[0] + 1 <= lz.products() <= its[0] + 5
+    o = so.SpmeOracle(g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
+    o.update(g["pos"])
+    yo, ito = so.block_lanczos_sqrt(lambda X: o.mulvec(X.T).T, z.T, 100, 1e-6)
+    assert ito > 0
+    assert rel_err(yo.T, y) < TOL
+    if reorth:
+        assert abs(its[0] - ito) <= 2, (its, ito)
+    # the same vector as the first column of a 2-RHS block agrees too
+    lz2 = sdt.BrwnLanczos(n3, 100, 2, 1e-8, reorth=reorth)
+    assert lz2.Init()
+    z2 = np.vstack([z, np.random.default_rng(10).standard_normal((1, n3))])
+    y2 = np.zeros((2, n3))
+    lz2.Compute(m, 2, n3, z2, n3, y2)
+    assert rel_err(y2[:1], y) < TOL
+
+
 def test_single_vector_and_groups(gpu_available):
     """nrhs = 1 takes the single-vector path; nrhs > max_nrhs is split into
     groups exactly as BrwnLanczos::Compute does; ldy > 3N is honoured."""

@@ -479,11 +479,12 @@ __global__ void k_sqnorm_partial(int n, int mb, const double *__restrict__ X, in
 //   k_vec_scale        V_{i+1} = W / sqrt(g) ; next W = B_i V_i
 // Cross-CTA sums: every CTA writes its partial sums and the last CTA to
 // arrive adds them in CTA order, so the results do not depend on scheduling.
-constexpr int kVecThreads = 256;
+constexpr int kVecThreads = 512;
+constexpr int kVecWarps = kVecThreads / 32;
 constexpr int kVecMaxRows = 2048;
 
-// Sum of v over the CTA, valid in thread 0; `red` holds 8 doubles and is
-// free again once every thread has returned.
+// Sum of v over the CTA, valid in thread 0; `red` holds kVecWarps doubles
+// and is free again once every thread has returned.
 __device__ __forceinline__ double vec_cta_sum(double v, double *red)
 {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -492,7 +493,7 @@ __device__ __forceinline__ double vec_cta_sum(double v, double *red)
     double t = 0.0;
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int w = 0; w < kVecThreads / 32; w++) t += red[w];
+        for (int w = 0; w < kVecWarps; w++) t += red[w];
     return t;
 }
 
@@ -509,26 +510,41 @@ __device__ __forceinline__ bool vec_last_cta(unsigned *arrive)
     return last != 0;
 }
 
-// out[j] = sum over CTAs q of part[q * ncol + j] (lanes take q mod 32, then
-// a fixed shuffle tree; lane 0's sum is stored).
-__device__ __forceinline__ void vec_fold(int ncol, const double *part, double *out)
+// out[j] = sum over CTAs q of part[q * ncol + j], by the whole CTA: up to
+// 32 threads per column take the CTAs q = g, g + groups, .. (eight loads in
+// flight each), and their sums are added in group order through `red`
+// (kVecThreads doubles).  Thread j < ncol stores out[j] (thread 0 for one
+// column).
+__device__ __forceinline__ void vec_fold(int ncol, const double *part, double *out, double *red)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int j = w; j < ncol; j += kVecThreads / 32) {
+    const int G = gridDim.x, t = threadIdx.x;
+    for (int j0 = 0; j0 < ncol; j0 += kVecThreads) {
+        const int nc = min(kVecThreads, ncol - j0);
+        const int groups = min(32, kVecThreads / nc);
+        const int j = t % nc, g = t / nc;
         double s = 0.0;
-        for (int q = lane; q < (int)gridDim.x; q += 32) s += __ldcg(&part[(size_t)q * ncol + j]);
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) out[j] = s;
+        if (g < groups) {
+#pragma unroll 8
+            for (int q = g; q < G; q += groups) s += __ldcg(&part[(size_t)q * ncol + j0 + j]);
+        }
+        red[t] = s;
+        __syncthreads();
+        if (t < nc) {
+            double a = 0.0;
+            for (int gg = 0; gg < groups; gg++) a += red[gg * nc + t];
+            out[j0 + t] = a;
+        }
+        __syncthreads();
     }
 }
 
 // The last CTA's normalisation factor from g = ||W||^2: B = sqrt(g) and
 // 1/B; a g that is not positive is a breakdown (flag 1, and 1/B = 0 so the
 // vector becomes zero and stays finite), as in chol_qr_step_warp.
-__device__ __forceinline__ void vec_norm_fold(const double *part, double *B, double *ri, double *flag)
+__device__ __forceinline__ void vec_norm_fold(const double *part, double *B, double *ri, double *flag, double *red)
 {
     double d = 0.0;
-    vec_fold(1, part, &d);  // the sum lands in thread 0
+    vec_fold(1, part, &d, red);  // the sum lands in thread 0
     if (threadIdx.x != 0) return;
     if (!(d > 0.0)) {
         *ri = 0.0;
@@ -546,20 +562,21 @@ __global__ void __launch_bounds__(kVecThreads)
 k_vec_dot(int n, int rows, const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ part,
           unsigned *__restrict__ arrive, double *__restrict__ out)
 {
-    __shared__ double red[kVecThreads / 32];
+    __shared__ double red[kVecThreads];
     const int e0 = blockIdx.x * rows, e1 = min(n, e0 + rows);
     double s = 0.0;
     for (int e = e0 + threadIdx.x; e < e1; e += kVecThreads) s = fma(x[e], y[e], s);
     s = vec_cta_sum(s, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (!vec_last_cta(arrive)) return;
-    vec_fold(1, part, out);
+    vec_fold(1, part, out, red);
     if (threadIdx.x == 0) *arrive = 0u;
 }
 
 // W -= a V_i (a = *pa, V_i = V + (ma - 1) ldv); c[j] = V_j . W for j < ma.
 // The CTA keeps its chunk of the new W in shared memory; warp w takes the
-// columns 4w..4w+3, 4w+32.. (four at a time, lanes over the rows).
+// columns 4w..4w+3, 4w+4 kVecWarps.. (four at a time) with the lanes over
+// the rows, four rows a lane at once (sixteen loads in flight).
 __global__ void __launch_bounds__(kVecThreads)
 k_vec_axpy_dots(int n, int rows, int ma, const double *__restrict__ V, int ldv, const double *__restrict__ pa,
                 double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
@@ -576,11 +593,25 @@ k_vec_axpy_dots(int n, int rows, int ma, const double *__restrict__ V, int ldv, 
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    for (int j0 = 4 * wp; j0 < ma; j0 += 4 * (kVecThreads / 32)) {
+    for (int j0 = 4 * wp; j0 < ma; j0 += 4 * kVecWarps) {
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         const double *Vj = V + (size_t)j0 * ldv + e0;
         const int nq = min(4, ma - j0);
-        for (int r = lane; r < len; r += 32) {
+        int r = lane;
+        for (; r + 96 < len; r += 128) {
+            double w[4], v[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) w[u] = sw[r + 32 * u];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+                for (int u = 0; u < 4; u++) v[q][u] = q < nq ? Vj[(size_t)q * ldv + r + 32 * u] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+                for (int u = 0; u < 4; u++) s[q] = fma(v[q][u], w[u], s[q]);
+        }
+        for (; r < len; r += 32) {
             const double w = sw[r];
 #pragma unroll
             for (int q = 0; q < 4; q++)
@@ -593,8 +624,7 @@ k_vec_axpy_dots(int n, int rows, int ma, const double *__restrict__ V, int ldv, 
         }
     }
     if (!vec_last_cta(arrive)) return;
-    vec_fold(ma, part, c);
-    __syncthreads();
+    vec_fold(ma, part, c, sw);
     if (threadIdx.x == 0) *arrive = 0u;
 }
 
@@ -604,7 +634,7 @@ k_vec_axpy_norm(int n, int rows, const double *__restrict__ Vi, const double *__
                 double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
                 double *__restrict__ B, double *__restrict__ ri, double *__restrict__ flag)
 {
-    __shared__ double red[kVecThreads / 32];
+    __shared__ double red[kVecThreads];
     const int e0 = blockIdx.x * rows, e1 = min(n, e0 + rows);
     const double a = *pa;
     double s = 0.0;
@@ -616,31 +646,48 @@ k_vec_axpy_norm(int n, int rows, const double *__restrict__ Vi, const double *__
     s = vec_cta_sum(s, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (!vec_last_cta(arrive)) return;
-    vec_norm_fold(part, B, ri, flag);
+    vec_norm_fold(part, B, ri, flag, red);
     if (threadIdx.x == 0) *arrive = 0u;
 }
 
 // W -= sum_{j < ma} V_j c[j]; B = ||W||, 1/B and the breakdown flag.  A
-// thread owns rows r, r + 256, .. of the chunk (at most 8).
+// thread owns rows r, r + kVecThreads, .. of the chunk (at most four) and
+// takes the columns eight at a time, their loads issued together.
 __global__ void __launch_bounds__(kVecThreads)
 k_vec_sub_norm(int n, int rows, int ma, const double *__restrict__ V, int ldv, const double *__restrict__ c,
                double *__restrict__ W, double *__restrict__ part, unsigned *__restrict__ arrive,
                double *__restrict__ B, double *__restrict__ ri, double *__restrict__ flag)
 {
     constexpr int R = kVecMaxRows / kVecThreads;
-    __shared__ double red[kVecThreads / 32];
+    constexpr int J = 8;
+    __shared__ double red[kVecThreads];
     const int e0 = blockIdx.x * rows, len = min(n, e0 + rows) - e0;
     double acc[R];
 #pragma unroll
     for (int m = 0; m < R; m++) acc[m] = 0.0;
-#pragma unroll 4
-    for (int j = 0; j < ma; j++) {
+    int j = 0;
+    for (; j + J <= ma; j += J) {
+        double cj[J], v[J][R];
+#pragma unroll
+        for (int u = 0; u < J; u++) cj[u] = __ldg(&c[j + u]);
+#pragma unroll
+        for (int u = 0; u < J; u++)
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                const int r = threadIdx.x + m * kVecThreads;
+                v[u][m] = r < len ? V[(size_t)(j + u) * ldv + e0 + r] : 0.0;
+            }
+#pragma unroll
+        for (int u = 0; u < J; u++)
+#pragma unroll
+            for (int m = 0; m < R; m++) acc[m] = fma(v[u][m], cj[u], acc[m]);
+    }
+    for (; j < ma; j++) {
         const double cj = __ldg(&c[j]);
-        const double *Vj = V + (size_t)j * ldv + e0;
 #pragma unroll
         for (int m = 0; m < R; m++) {
             const int r = threadIdx.x + m * kVecThreads;
-            if (r < len) acc[m] = fma(Vj[r], cj, acc[m]);
+            if (r < len) acc[m] = fma(V[(size_t)j * ldv + e0 + r], cj, acc[m]);
         }
     }
     double s = 0.0;
@@ -656,7 +703,7 @@ k_vec_sub_norm(int n, int rows, int ma, const double *__restrict__ V, int ldv, c
     s = vec_cta_sum(s, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (!vec_last_cta(arrive)) return;
-    vec_norm_fold(part, B, ri, flag);
+    vec_norm_fold(part, B, ri, flag, red);
     if (threadIdx.x == 0) *arrive = 0u;
 }
 
@@ -670,6 +717,282 @@ k_vec_scale(int n, const double *__restrict__ ri, double *__restrict__ W, const 
     if (e >= n) return;
     W[e] *= *ri;
     if (Wn) Wn[e] = *B * Vi[e];
+}
+
+// ---------------------------------------------------------------------------
+// The whole single-vector iteration in one cooperative launch: the four
+// steps above as phases of one kernel, separated by grid barriers instead of
+// kernel boundaries.  A CTA takes the row chunks blockIdx.x, blockIdx.x + G,
+// .. (G = gridDim.x, all CTAs resident), writes one partial sum per phase
+// and column, and after the barrier every CTA adds all G partials itself in
+// the same fixed order, so every CTA holds the same A_i, c and B_i to the
+// bit.  Barrier counters: bar[p] for this launch (p = launch parity), while
+// CTA 0 clears bar[p ^ 1] for the next one (the launch before this one, which
+// used it, has completed).  A barrier wait gives up after about a second
+// (kVecSpinLimit polls), sets *err and returns; the host reports it.
+constexpr int kVecMaxCols = 512;           // columns the fused kernel stages in shared memory
+constexpr long long kVecSpinLimit = 1 << 21;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Arrive at the grid barrier and wait until `target` CTAs have arrived in
+// total; false (in every thread) when the wait gave up.
+__device__ __forceinline__ bool vec_grid_sync(unsigned *bar, unsigned target, unsigned *err)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        atomicAdd(bar, 1u);
+        long long spins = 0;
+        while (ld_acquire_u32(bar) < target) {
+            if (++spins > kVecSpinLimit) {
+                atomicOr(err, 1u);
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Sum of part[0 .. G) in a fixed order, by one warp: a lane loads q = lane,
+// lane + 32, .. (all eight of a 256-block issued together) and adds them in
+// order, then a fixed shuffle tree; every lane returns lane 0's sum.
+__device__ __forceinline__ double vec_warp_sum_parts(const double *part, int G)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int q0 = 0; q0 < G; q0 += 256) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int q = q0 + lane + 32 * u;
+            v[u] = q < G ? __ldcg(&part[q]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) s += v[u];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return __shfl_sync(0xffffffffu, s, 0);
+}
+
+// part: [G] dot partials, [ma][G] reorthogonalisation partials (column-major,
+// so a column's partials are contiguous for the fold), [G] norm partials.
+// Wn as k_vec_scale.  dA/dB/dflag: the iteration's history slots (written
+// by CTA 0).  While the first barrier is pending, the CTA's rows of
+// V_0 .. V_{i-1} are prefetched into L2 (the mobility product in between
+// has streamed far more than L2 holds), so the reorthogonalisation reads
+// them from there.
+__global__ void __launch_bounds__(kVecThreads, 1)
+k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__restrict__ V, int ldv,
+           double *__restrict__ Wn, double *__restrict__ part, unsigned *__restrict__ bars, int parity,
+           unsigned *__restrict__ err, double *__restrict__ dA, double *__restrict__ dB, double *__restrict__ dflag)
+{
+    __shared__ double sw[kVecMaxRows];
+    __shared__ double sc[kVecMaxCols];
+    __shared__ double red[kVecWarps];
+    __shared__ double sval[2];
+    const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    unsigned *bar = bars + parity;
+    if (blockIdx.x == 0 && tid == 0) bars[parity ^ 1] = 0u;
+    const double *Vi = V + (size_t)(ma - 1) * ldv;
+    double *W = const_cast<double *>(Vi) + ldv;
+    double *p1 = part, *p2 = part + G, *p3 = p2 + (size_t)G * ma;
+
+    // A_i = V_i . W
+    double s = 0.0;
+    for (int ch = blockIdx.x; ch < nchunks; ch += G) {
+        const int e1 = min(n, (ch + 1) * rows);
+        for (int e = ch * rows + tid; e < e1; e += kVecThreads) s = fma(Vi[e], W[e], s);
+    }
+    if (reorth) {
+        // 128-byte lines of the chunks' rows of V_0 .. V_{i-1}
+        for (int ch = blockIdx.x; ch < nchunks; ch += G) {
+            const int e0 = ch * rows, e1 = min(n, e0 + rows);
+            const int l0 = e0 / 16, nl = (e1 - 1) / 16 - l0 + 1;
+            for (int t = tid; t < (ma - 1) * nl; t += kVecThreads) {
+                const int j = t / nl, l = l0 + t % nl;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(V + (size_t)j * ldv + 16 * l));
+            }
+        }
+    }
+    s = vec_cta_sum(s, red);
+    if (tid == 0) p1[blockIdx.x] = s;
+    if (!vec_grid_sync(bar, G, err)) return;
+    if (wp == 0) {
+        const double a = vec_warp_sum_parts(p1, G);
+        if (lane == 0) {
+            sval[0] = a;
+            if (blockIdx.x == 0) *dA = a;
+        }
+    }
+    __syncthreads();
+    const double a = sval[0];
+
+    // W -= A_i V_i, then either c = V_{0..i}^T W or g = W . W
+    s = 0.0;
+    bool first = true;
+    for (int ch = blockIdx.x; ch < nchunks; ch += G) {
+        const int e0 = ch * rows, len = min(n, e0 + rows) - e0;
+        __syncthreads();  // sw is free again
+        for (int r = tid; r < len; r += kVecThreads) {
+            const double w = fma(-a, Vi[e0 + r], W[e0 + r]);
+            W[e0 + r] = w;
+            if (reorth) sw[r] = w;
+            else s = fma(w, w, s);
+        }
+        if (!reorth) continue;
+        __syncthreads();
+        // warp wp: columns j0 .. j0+3; a lane takes rows lane, lane + 32, ..,
+        // eight of them (32 loads) at a time
+        for (int j0 = 4 * wp; j0 < ma; j0 += 4 * kVecWarps) {
+            double t[4] = {0.0, 0.0, 0.0, 0.0};
+            const double *Vj = V + (size_t)j0 * ldv + e0;
+            const int nq = min(4, ma - j0);
+            for (int r0 = 0; r0 < len; r0 += 256) {
+                double w[8], v[4][8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int r = r0 + lane + 32 * u;
+                    w[u] = r < len ? sw[r] : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int r = r0 + lane + 32 * u;
+                        v[q][u] = (q < nq && r < len) ? Vj[(size_t)q * ldv + r] : 0.0;
+                    }
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+#pragma unroll
+                    for (int u = 0; u < 8; u++) t[q] = fma(v[q][u], w[u], t[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                for (int o = 16; o > 0; o >>= 1) t[q] += __shfl_xor_sync(0xffffffffu, t[q], o);
+                // lane 0 of the warp that owns column j0 + q accumulates this CTA's chunks
+                if (lane == 0 && q < nq) {
+                    double *dst = &p2[(size_t)(j0 + q) * G + blockIdx.x];
+                    *dst = first ? t[q] : *dst + t[q];
+                }
+            }
+        }
+        first = false;
+    }
+    unsigned target = 2u * G;
+    if (reorth) {
+        if (first)  // a CTA without chunks contributes zeros
+            for (int j = tid; j < ma; j += kVecThreads) p2[(size_t)j * G + blockIdx.x] = 0.0;
+        if (!vec_grid_sync(bar, target, err)) return;
+        target += G;
+        // c_j = sum over CTAs (warp w takes the columns j = w mod kVecWarps)
+        for (int j = wp; j < ma; j += kVecWarps) {
+            const double c = vec_warp_sum_parts(p2 + (size_t)j * G, G);
+            if (lane == 0) sc[j] = c;
+        }
+        __syncthreads();
+        // W -= V_{0..i} c ; g = W . W
+        s = 0.0;
+        for (int ch = blockIdx.x; ch < nchunks; ch += G) {
+            const int e0 = ch * rows, len = min(n, e0 + rows) - e0;
+            if (len <= kVecThreads) {
+                // one row a thread: sixteen columns' loads at a time
+                constexpr int J = 16;
+                const int r = tid;
+                if (r < len) {
+                    const double *Vr = V + e0 + r;
+                    double acc = 0.0;
+                    int j = 0;
+                    for (; j + J <= ma; j += J) {
+                        double v[J];
+#pragma unroll
+                        for (int u = 0; u < J; u++) v[u] = Vr[(size_t)(j + u) * ldv];
+#pragma unroll
+                        for (int u = 0; u < J; u++) acc = fma(v[u], sc[j + u], acc);
+                    }
+                    for (; j < ma; j++) acc = fma(Vr[(size_t)j * ldv], sc[j], acc);
+                    const double w = W[e0 + r] - acc;
+                    W[e0 + r] = w;
+                    s = fma(w, w, s);
+                }
+                continue;
+            }
+            constexpr int R = kVecMaxRows / kVecThreads;
+            constexpr int J = 8;
+            double acc[R];
+#pragma unroll
+            for (int m = 0; m < R; m++) acc[m] = 0.0;
+            int j = 0;
+            for (; j + J <= ma; j += J) {
+                double v[J][R];
+#pragma unroll
+                for (int u = 0; u < J; u++)
+#pragma unroll
+                    for (int m = 0; m < R; m++) {
+                        const int r = tid + m * kVecThreads;
+                        v[u][m] = r < len ? V[(size_t)(j + u) * ldv + e0 + r] : 0.0;
+                    }
+#pragma unroll
+                for (int u = 0; u < J; u++)
+#pragma unroll
+                    for (int m = 0; m < R; m++) acc[m] = fma(v[u][m], sc[j + u], acc[m]);
+            }
+            for (; j < ma; j++) {
+#pragma unroll
+                for (int m = 0; m < R; m++) {
+                    const int r = tid + m * kVecThreads;
+                    if (r < len) acc[m] = fma(V[(size_t)j * ldv + e0 + r], sc[j], acc[m]);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                const int r = tid + m * kVecThreads;
+                if (r < len) {
+                    const double w = W[e0 + r] - acc[m];
+                    W[e0 + r] = w;
+                    s = fma(w, w, s);
+                }
+            }
+        }
+    }
+    s = vec_cta_sum(s, red);
+    if (tid == 0) p3[blockIdx.x] = s;
+    if (!vec_grid_sync(bar, target, err)) return;
+    // B_i = ||W||, as vec_norm_fold
+    if (wp == 0) {
+        const double d = vec_warp_sum_parts(p3, G);
+        if (lane == 0) {
+            const bool ok = d > 0.0;
+            const double b = ok ? sqrt(d) : 0.0;
+            sval[0] = b;
+            sval[1] = ok ? 1.0 / b : 0.0;
+            if (blockIdx.x == 0) {
+                *dB = b;
+                *dflag = ok ? 0.0 : 1.0;
+            }
+        }
+    }
+    __syncthreads();
+    const double b = sval[0], ri = sval[1];
+    // V_{i+1} = W / B_i ; next W = B_i V_i
+    for (int ch = blockIdx.x; ch < nchunks; ch += G) {
+        const int e1 = min(n, (ch + 1) * rows);
+        for (int e = ch * rows + tid; e < e1; e += kVecThreads) {
+            W[e] *= ri;
+            if (Wn) Wn[e] = b * Vi[e];
+        }
+    }
 }
 
 // x *= s (host scalar)
@@ -787,7 +1110,7 @@ static int upload(LanczosState *lz, double *d, const double *h, size_t count)
 static int vec_rows(int n, int num_sms)
 {
     const int per = (n + num_sms - 1) / std::max(1, num_sms);
-    return std::min(kVecMaxRows, std::max(kVecThreads, (per + 31) / 32 * 32));
+    return std::min(kVecMaxRows, std::max(256, (per + 31) / 32 * 32));
 }
 
 // One Cholesky-QR step of one k x k Gram matrix (chol_qr_step_warp), one warp.
@@ -843,10 +1166,27 @@ int lanczos_alloc(LanczosState *lz)
     lz->part_cap = std::max((size_t)lz->gram_chunks * 16 * 16, (size_t)64 * mmax * lz->max_nrhs);
     // the single-vector kernels' per-chunk partial sums of up to mmax columns
     const int vrows = vec_rows(lz->dim, lz->num_sms);
-    lz->part_cap = std::max(lz->part_cap, (size_t)((lz->dim + vrows - 1) / vrows) * mmax);
+    lz->part_cap = std::max(lz->part_cap, (size_t)((lz->dim + vrows - 1) / vrows) * (mmax + 2));
     LZ_CUDA(cudaMalloc(&lz->d_part, lz->part_cap * sizeof(double)));
-    LZ_CUDA(cudaMalloc(&lz->d_arrive, sizeof(unsigned)));
-    LZ_CUDA(cudaMemset(lz->d_arrive, 0, sizeof(unsigned)));
+    // [0] last-CTA counter of the Gram folds, [1..2] grid-barrier counters of
+    // the fused single-vector iteration, [3] its barrier-timeout flag
+    LZ_CUDA(cudaMalloc(&lz->d_arrive, 4 * sizeof(unsigned)));
+    LZ_CUDA(cudaMemset(lz->d_arrive, 0, 4 * sizeof(unsigned)));
+    LZ_CUDA(cudaMallocHost(&lz->h_err, sizeof(unsigned)));
+    *lz->h_err = 0u;
+    // the fused single-vector iteration: one resident CTA per row chunk at most
+    // (STOKESDT_VEC_UNFUSED=1 keeps the four-launch form)
+    {
+        int coop = 0, per_sm = 0;
+        lz->vec_grid = 0;
+        const char *unfused = std::getenv("STOKESDT_VEC_UNFUSED");
+        if (!(unfused && unfused[0] == '1') &&
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, lz->device) == cudaSuccess && coop &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vec_iter, kVecThreads, 0) == cudaSuccess &&
+            per_sm > 0)
+            lz->vec_grid = std::min(per_sm * lz->num_sms, (lz->dim + vrows - 1) / vrows);
+        cudaGetLastError();
+    }
     LZ_CUDA(cudaMalloc(&lz->d_small, (size_t)mmax * std::max(lz->max_nrhs, 16) * sizeof(double)));
     LZ_CUDA(cudaMalloc(&lz->d_coef, (size_t)mmax * lz->max_nrhs * sizeof(double)));
     LZ_CUDA(cudaMalloc(&lz->d_dY, (size_t)lz->max_nrhs * lz->ldv * sizeof(double)));
@@ -871,6 +1211,8 @@ void lanczos_free(LanczosState *lz)
         if (q) cudaFree(q);
     if (lz->h_hist) cudaFreeHost(lz->h_hist);
     lz->h_hist = nullptr;
+    if (lz->h_err) cudaFreeHost(lz->h_err);
+    lz->h_err = nullptr;
     for (cudaEvent_t e : lz->ev)
         if (e) cudaEventDestroy(e);
     lz->ev.clear();
@@ -934,6 +1276,23 @@ static int vec_iteration(LanczosState *lz, int it, double *V, double *Wn, double
     const int rows = vec_rows(n, lz->num_sms), grid = (n + rows - 1) / rows;
     double *Vi = V + (size_t)it * ldv, *W = Vi + ldv;
     double *ri = lz->d_qr;
+    int ma = it + 1;
+    if (lz->vec_grid > 0 && ma <= kVecMaxCols) {
+        // one cooperative launch (all CTAs resident: they wait on one another)
+        int nchunks = grid, rev = reorth ? 1 : 0, parity = (int)(lz->vec_launches & 1);
+        double *part = lz->d_part;
+        unsigned *bars = lz->d_arrive + 1, *err = lz->d_arrive + 3;
+        void *args[] = {(void *)&n, (void *)&rows, (void *)&nchunks, (void *)&ma, (void *)&rev, (void *)&V,
+                        (void *)&ldv, (void *)&Wn, (void *)&part, (void *)&bars, (void *)&parity, (void *)&err,
+                        (void *)&dA, (void *)&dB, (void *)&dflag};
+        pt.begin(1);
+        LZ_CUDA(cudaLaunchCooperativeKernel((const void *)k_vec_iter, dim3(lz->vec_grid), dim3(kVecThreads), args, 0,
+                                            lz->stream));
+        LZ_LAUNCH();
+        pt.end();
+        lz->vec_launches++;
+        return kOk;
+    }
     pt.begin(1);
     k_vec_dot<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, Vi, W, lz->d_part, lz->d_arrive, dA);
     LZ_LAUNCH();
@@ -1014,6 +1373,7 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
         int status = 0, neg = 0;
         bool breakdown = false;
         double ms = 0.0;
+        Clock::time_point ready;  // when the iteration's coefficients had arrived
         std::vector<double> D;
     };
     std::atomic<bool> cancel{false};
@@ -1025,6 +1385,7 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
             return out;
         }
         const Clock::time_point t0 = Clock::now();
+        out.ready = t0;
         const int m = (it + 1) * k;
         const double *h = lz->h_hist;
         out.breakdown = h[(size_t)it * hs + 2 * kk] != 0.0;
@@ -1119,11 +1480,15 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
     // The last checked errors decay geometrically; iteration j is expected to
     // pass the test when the extrapolated error is below tol.  Issuing work
     // past that point would only be discarded, so the host then waits for the
-    // outstanding checks before it issues more.
+    // outstanding checks before it issues more.  The rate is the mean over
+    // the last (up to six) checks: with one vector the error falls by ratios
+    // anywhere from 0.3 to 1.4 from one check to the next, so the last ratio
+    // alone often predicts no convergence at all.
     auto expect_converged = [&](int j) {
         const std::vector<double> &h = lz->history;
         if (h.size() < 2 || done_it < 0) return false;
-        const double q = h.back() / h[h.size() - 2];
+        const int w = std::min<int>(6, (int)h.size() - 1);
+        const double q = std::pow(h.back() / h[h.size() - 1 - w], 1.0 / w);
         if (!(q > 0.0) || q >= 1.0) return false;
         return h.back() * std::pow(q, (double)(j - done_it)) < lz->tol;
     };
@@ -1137,15 +1502,31 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
     // may be in flight; without it the check issues device work on the solver
     // stream, so one solve is in flight.  Work issued past the converged
     // iteration is discarded.
+    //
+    // Every solve in flight is an iteration that may run past convergence, so
+    // only as many are kept as cover the host's solve: two, plus one per
+    // GPU iteration time the last solve took (at most `lookahead`).  The GPU
+    // iteration time is the gap between the arrivals of consecutive
+    // iterations' coefficients.
     std::deque<std::pair<int, std::future<Solved>>> pending;
-    const int lookahead = reorth ? std::max(1, lz->lookahead) : 1;
+    const int lookahead_max = reorth ? std::max(1, lz->lookahead) : 1;
+    int lookahead = lookahead_max;
     int it;
+    int last_ready_it = -2;
+    Clock::time_point last_ready;
     auto take_front = [&]() -> int {
         const Clock::time_point tw = Clock::now();
         Solved sv = pending.front().second.get();
         lz->t_wait_ms += ms_since(tw);
         const int i = pending.front().first;
         pending.pop_front();
+        if (sv.status == 0 && last_ready_it == i - 1) {
+            const double t_iter = std::chrono::duration<double, std::milli>(sv.ready - last_ready).count();
+            if (t_iter > 0.0)
+                lookahead = std::min(lookahead_max, 2 + (int)std::floor(sv.ms / t_iter));
+        }
+        last_ready_it = i;
+        last_ready = sv.ready;
         return check(i, std::move(sv));
     };
     PhaseTimer pt;
@@ -1228,8 +1609,16 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
     if (st != kOk) return st;
     // Y = V_{0..i} D_i
     const int mfinal = (done_it + 1) * k;
+    if (k == 1 && lz->vec_grid > 0)  // arrives with the upload's synchronisation
+        LZ_CUDA(cudaMemcpyAsync(lz->h_err, lz->d_arrive + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, lz->stream));
     st = upload(lz, lz->d_coef, D.data(), D.size());
     if (st != kOk) return st;
+    if (k == 1 && lz->vec_grid > 0 && *lz->h_err != 0u) {
+        *lz->h_err = 0u;
+        LZ_CUDA(cudaMemsetAsync(lz->d_arrive, 0, 4 * sizeof(unsigned), lz->stream));
+        lz->last_error = "single-vector iteration: a grid barrier wait timed out";
+        return kErrCuda;
+    }
     st = block_gemm(lz, mfinal, V, ldv, lz->d_coef, k, 0.0, d_y, ldy);
     if (st != kOk) return st;
     *iters_out = converged ? done_it : -1;

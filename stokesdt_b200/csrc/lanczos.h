@@ -16,12 +16,15 @@ struct LanczosState {
     int dim = 0, max_iters = 0, max_nrhs = 0;
     double tol = 0.0;
     bool reorth = false;        // the reference does not reorthogonalise
-    int lookahead = 4;          // eigensolves in flight with reorthogonalisation
+    int lookahead = 4;          // most eigensolves in flight with reorthogonalisation
     int ldv = 0;
     double *d_V = nullptr;      // Krylov basis [(max_iters+1) * k][ldv]
     double *d_part = nullptr;   // Gram partial sums
     unsigned *d_arrive = nullptr;  // CTAs done with a small Gram (the last one sums the parts)
     size_t part_cap = 0;
+    int vec_grid = 0;                  // CTAs of the fused single-vector iteration (0: not available)
+    unsigned long long vec_launches = 0;  // its launches so far (their parity picks the barrier counter)
+    unsigned *h_err = nullptr;         // pinned copy of its barrier-timeout flag
     int gram_chunks = 0;
     int num_sms = 148;
     double *d_small = nullptr;  // k x k scratch

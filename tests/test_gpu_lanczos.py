@@ -84,13 +84,17 @@ def test_block_lanczos_vs_oracle_config1(gpu_available):
     assert rel_err(Yo.T, Y) < TOL
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("reorth", [True, False])
-def test_single_vector_vs_oracle_config1(gpu_available, reorth):
-    """One RHS (the dot-product/axpy iteration, one normalisation per step)
-    against the FP64 oracle's Lanczos on the FP64 oracle SPME, config 1, tol
-    1e-6.  With reorthogonalisation the basis stays orthonormal, so the
-    iteration count matches the oracle's to within the checks issued ahead."""
+def test_single_vector_vs_oracle_config1(gpu_available, reorth, fused, monkeypatch):
+    """One RHS (the dot-product/axpy iteration, one normalisation per step;
+    fused: one cooperative launch per iteration, else four launches) against
+    the FP64 oracle's Lanczos on the FP64 oracle SPME, config 1, tol 1e-6.
+    With reorthogonalisation the basis stays orthonormal, so the iteration
+    count matches the oracle's to within the checks issued ahead."""
     import stokesdt_b200 as sdt
+    if not fused:
+        monkeypatch.setenv("STOKESDT_VEC_UNFUSED", "1")
     from oracle import spme_oracle as so
     g = golden("spme_cfg1")
     N = len(g["rdi"])

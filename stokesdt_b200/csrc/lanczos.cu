@@ -796,7 +796,8 @@ __device__ __forceinline__ double vec_warp_sum_parts(const double *part, int G)
 __global__ void __launch_bounds__(kVecThreads, 1)
 k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__restrict__ V, int ldv,
            double *__restrict__ Wn, double *__restrict__ part, unsigned *__restrict__ bars, int parity,
-           unsigned *__restrict__ err, double *__restrict__ dA, double *__restrict__ dB, double *__restrict__ dflag)
+           unsigned skew, unsigned *__restrict__ err, double *__restrict__ dA, double *__restrict__ dB,
+           double *__restrict__ dflag)
 {
     __shared__ double sw[kVecMaxRows];
     __shared__ double sc[kVecMaxCols];
@@ -808,6 +809,15 @@ k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__res
     const double *Vi = V + (size_t)(ma - 1) * ldv;
     double *W = const_cast<double *>(Vi) + ldv;
     double *p1 = part, *p2 = part + G, *p3 = p2 + (size_t)G * ma;
+    // after a wait that ran out: the iteration reads as a breakdown, so the
+    // host stops issuing, and the flag in *err reports it
+    auto give_up = [&]() {
+        if (blockIdx.x == 0 && tid == 0) {
+            *dA = 0.0;
+            *dB = 0.0;
+            *dflag = 1.0;
+        }
+    };
 
     // A_i = V_i . W
     double s = 0.0;
@@ -828,7 +838,7 @@ k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__res
     }
     s = vec_cta_sum(s, red);
     if (tid == 0) p1[blockIdx.x] = s;
-    if (!vec_grid_sync(bar, G, err)) return;
+    if (!vec_grid_sync(bar, G + skew, err)) return give_up();
     if (wp == 0) {
         const double a = vec_warp_sum_parts(p1, G);
         if (lane == 0) {
@@ -894,7 +904,7 @@ k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__res
     if (reorth) {
         if (first)  // a CTA without chunks contributes zeros
             for (int j = tid; j < ma; j += kVecThreads) p2[(size_t)j * G + blockIdx.x] = 0.0;
-        if (!vec_grid_sync(bar, target, err)) return;
+        if (!vec_grid_sync(bar, target, err)) return give_up();
         target += G;
         // c_j = sum over CTAs (warp w takes the columns j = w mod kVecWarps)
         for (int j = wp; j < ma; j += kVecWarps) {
@@ -968,7 +978,7 @@ k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__res
     }
     s = vec_cta_sum(s, red);
     if (tid == 0) p3[blockIdx.x] = s;
-    if (!vec_grid_sync(bar, target, err)) return;
+    if (!vec_grid_sync(bar, target, err)) return give_up();
     // B_i = ||W||, as vec_norm_fold
     if (wp == 0) {
         const double d = vec_warp_sum_parts(p3, G);
@@ -1180,6 +1190,11 @@ int lanczos_alloc(LanczosState *lz)
         int coop = 0, per_sm = 0;
         lz->vec_grid = 0;
         const char *unfused = std::getenv("STOKESDT_VEC_UNFUSED");
+        // STOKESDT_VEC_BARRIER_SKEW=k raises the first barrier's target by k
+        // arrivals that never come: the wait runs out, which the failure
+        // tests use to check that it is reported
+        const char *skew = std::getenv("STOKESDT_VEC_BARRIER_SKEW");
+        lz->vec_barrier_skew = skew ? (unsigned)std::max(0, std::atoi(skew)) : 0u;
         if (!(unfused && unfused[0] == '1') &&
             cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, lz->device) == cudaSuccess && coop &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vec_iter, kVecThreads, 0) == cudaSuccess &&
@@ -1280,18 +1295,27 @@ static int vec_iteration(LanczosState *lz, int it, double *V, double *Wn, double
     if (lz->vec_grid > 0 && ma <= kVecMaxCols) {
         // one cooperative launch (all CTAs resident: they wait on one another)
         int nchunks = grid, rev = reorth ? 1 : 0, parity = (int)(lz->vec_launches & 1);
+        unsigned skew = lz->vec_barrier_skew;
         double *part = lz->d_part;
         unsigned *bars = lz->d_arrive + 1, *err = lz->d_arrive + 3;
         void *args[] = {(void *)&n, (void *)&rows, (void *)&nchunks, (void *)&ma, (void *)&rev, (void *)&V,
-                        (void *)&ldv, (void *)&Wn, (void *)&part, (void *)&bars, (void *)&parity, (void *)&err,
-                        (void *)&dA, (void *)&dB, (void *)&dflag};
+                        (void *)&ldv, (void *)&Wn, (void *)&part, (void *)&bars, (void *)&parity, (void *)&skew,
+                        (void *)&err, (void *)&dA, (void *)&dB, (void *)&dflag};
         pt.begin(1);
-        LZ_CUDA(cudaLaunchCooperativeKernel((const void *)k_vec_iter, dim3(lz->vec_grid), dim3(kVecThreads), args, 0,
-                                            lz->stream));
-        LZ_LAUNCH();
-        pt.end();
-        lz->vec_launches++;
-        return kOk;
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_vec_iter, dim3(lz->vec_grid),
+                                                          dim3(kVecThreads), args, 0, lz->stream);
+        if (e == cudaErrorCooperativeLaunchTooLarge) {
+            // fewer SMs than measured at allocation (a shared device): the
+            // four-launch form from now on
+            cudaGetLastError();
+            lz->vec_grid = 0;
+        } else {
+            LZ_CUDA(e);
+            LZ_LAUNCH();
+            pt.end();
+            lz->vec_launches++;
+            return kOk;
+        }
     }
     pt.begin(1);
     k_vec_dot<<<grid, kVecThreads, 0, lz->stream>>>(n, rows, Vi, W, lz->d_part, lz->d_arrive, dA);
@@ -1606,19 +1630,23 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
         pending.front().second.wait();
         pending.pop_front();
     }
+    if (k == 1) {
+        // a grid-barrier wait of the fused iteration that ran out voids the
+        // result, whatever the checks made of it
+        LZ_CUDA(cudaMemcpyAsync(lz->h_err, lz->d_arrive + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, lz->stream));
+        LZ_CUDA(cudaStreamSynchronize(lz->stream));
+        if (*lz->h_err != 0u) {
+            *lz->h_err = 0u;
+            LZ_CUDA(cudaMemsetAsync(lz->d_arrive, 0, 4 * sizeof(unsigned), lz->stream));
+            lz->last_error = "single-vector iteration: a grid barrier wait timed out";
+            return kErrCuda;
+        }
+    }
     if (st != kOk) return st;
     // Y = V_{0..i} D_i
     const int mfinal = (done_it + 1) * k;
-    if (k == 1 && lz->vec_grid > 0)  // arrives with the upload's synchronisation
-        LZ_CUDA(cudaMemcpyAsync(lz->h_err, lz->d_arrive + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, lz->stream));
     st = upload(lz, lz->d_coef, D.data(), D.size());
     if (st != kOk) return st;
-    if (k == 1 && lz->vec_grid > 0 && *lz->h_err != 0u) {
-        *lz->h_err = 0u;
-        LZ_CUDA(cudaMemsetAsync(lz->d_arrive, 0, 4 * sizeof(unsigned), lz->stream));
-        lz->last_error = "single-vector iteration: a grid barrier wait timed out";
-        return kErrCuda;
-    }
     st = block_gemm(lz, mfinal, V, ldv, lz->d_coef, k, 0.0, d_y, ldy);
     if (st != kOk) return st;
     *iters_out = converged ? done_it : -1;

@@ -24,6 +24,7 @@ struct LanczosState {
     size_t part_cap = 0;
     int vec_grid = 0;                  // CTAs of the fused single-vector iteration (0: not available)
     unsigned long long vec_launches = 0;  // its launches so far (their parity picks the barrier counter)
+    unsigned vec_barrier_skew = 0;     // arrivals added to its first barrier's target (failure tests only)
     unsigned *h_err = nullptr;         // pinned copy of its barrier-timeout flag
     int gram_chunks = 0;
     int num_sms = 148;

@@ -125,6 +125,40 @@ def test_single_vector_vs_oracle_config1(gpu_available, reorth, fused, monkeypat
     assert rel_err(y2[:1], y) < TOL
 
 
+def test_single_vector_barrier_timeout_reported(gpu_available, monkeypatch):
+    """A grid-barrier wait of the fused single-vector iteration that runs out
+    is reported, not hung on: STOKESDT_VEC_BARRIER_SKEW raises the first
+    barrier's target by one arrival that never comes, every CTA's bounded
+    wait gives up (about a second), the iteration reads as a breakdown and
+    Compute raises.  The context stays usable: a solver made afterwards
+    without the skew gives the result of one made before it (to the
+    rounding of the FP32 atomics' order in the products)."""
+    import stokesdt_b200 as sdt
+    g = golden("spme_cfg1")
+    N = len(g["rdi"])
+    n3 = 3 * N
+    m = sdt.MobSpme(N, g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
+    assert m.Init()
+    m.Update(g["pos"])
+    z = np.random.default_rng(11).standard_normal((1, n3))
+    y0 = np.zeros((1, n3))
+    lz0 = sdt.BrwnLanczos(n3, 100, 1, 1e-6, reorth=True)
+    assert lz0.Init()
+    lz0.Compute(m, 1, n3, z, n3, y0)
+    monkeypatch.setenv("STOKESDT_VEC_BARRIER_SKEW", "1")
+    lz = sdt.BrwnLanczos(n3, 3, 1, 1e-6, reorth=True)
+    assert lz.Init()
+    y = np.zeros((1, n3))
+    with pytest.raises(sdt.StokesError, match="grid barrier"):
+        lz.Compute(m, 1, n3, z, n3, y)
+    monkeypatch.delenv("STOKESDT_VEC_BARRIER_SKEW")
+    lz1 = sdt.BrwnLanczos(n3, 100, 1, 1e-6, reorth=True)
+    assert lz1.Init()
+    y1 = np.zeros((1, n3))
+    lz1.Compute(m, 1, n3, z, n3, y1)
+    assert rel_err(y0, y1) < 1e-6
+
+
 def test_single_vector_and_groups(gpu_available):
     """nrhs = 1 takes the single-vector path; nrhs > max_nrhs is split into
     groups exactly as BrwnLanczos::Compute does; ldy > 3N is honoured."""

@@ -13,8 +13,9 @@
 // is formed on the device every iteration exactly as the reference does
 // (brwn_lanczos.cc:181-196).  The QR of the reference (dgeqrf/dorgqr) and the
 // Cholesky QR used here differ only by column signs, which leave Y unchanged.
-// A block of one vector (k = 1) runs the same recurrence on dot-product and
-// axpy kernels, four launches per iteration (k_vec_*).
+// A block of one vector (k = 1) runs the same recurrence as dot products and
+// axpys, the whole iteration after the product in one cooperative launch
+// (k_vec_iter).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -469,16 +470,19 @@ __global__ void k_sqnorm_partial(int n, int mb, const double *__restrict__ X, in
 // Single-vector iteration (k = 1).  With one RHS every Gram matrix is a dot
 // product, every block product an axpy and the Cholesky QR a normalisation
 // (one pass: the second pass of a one-column Cholesky QR divides by
-// 1 + O(eps)), so an iteration's work after the mobility product takes four
-// launches over row chunks of `rows` (<= kVecMaxRows, one CTA each) instead
-// of the block path's eleven:
+// 1 + O(eps)).  By default an iteration's work after the mobility product
+// is one cooperative launch, k_vec_iter (below); the four-launch form over
+// row chunks of `rows` (<= kVecMaxRows, one CTA each) is the fallback where
+// a cooperative launch is not available (and STOKESDT_VEC_UNFUSED=1):
 //   k_vec_dot          A_i = V_i . W
 //   k_vec_axpy_dots    W -= A_i V_i ; c = V_{0..i}^T W      (reorthogonalised)
 //   k_vec_axpy_norm    W -= A_i V_i ; g = W . W             (without)
 //   k_vec_sub_norm     W -= V_{0..i} c ; g = W . W
 //   k_vec_scale        V_{i+1} = W / sqrt(g) ; next W = B_i V_i
-// Cross-CTA sums: every CTA writes its partial sums and the last CTA to
-// arrive adds them in CTA order, so the results do not depend on scheduling.
+// Either way the block path's eleven launches per iteration are gone.
+// Cross-CTA sums of the four-launch form: every CTA writes its partial sums
+// and the last CTA to arrive adds them in a fixed order, so the results do
+// not depend on scheduling.
 constexpr int kVecThreads = 512;
 constexpr int kVecWarps = kVecThreads / 32;
 constexpr int kVecMaxRows = 2048;

@@ -1634,23 +1634,26 @@ static int block_lanczos(LanczosState *lz, const MobOp &mob, int k, int ldz, con
         pending.front().second.wait();
         pending.pop_front();
     }
-    if (k == 1) {
-        // a grid-barrier wait of the fused iteration that ran out voids the
-        // result, whatever the checks made of it
+    // A grid-barrier wait of the fused single-vector iteration that ran out
+    // voids the result, whatever the checks made of it; its flag comes back
+    // with the synchronisation of the coefficient upload (or of the stream,
+    // when the iteration failed otherwise).
+    if (k == 1)
         LZ_CUDA(cudaMemcpyAsync(lz->h_err, lz->d_arrive + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, lz->stream));
+    const int mfinal = (done_it + 1) * k;
+    if (st == kOk) {
+        st = upload(lz, lz->d_coef, D.data(), D.size());
+    } else if (k == 1) {
         LZ_CUDA(cudaStreamSynchronize(lz->stream));
-        if (*lz->h_err != 0u) {
-            *lz->h_err = 0u;
-            LZ_CUDA(cudaMemsetAsync(lz->d_arrive, 0, 4 * sizeof(unsigned), lz->stream));
-            lz->last_error = "single-vector iteration: a grid barrier wait timed out";
-            return kErrCuda;
-        }
+    }
+    if (k == 1 && *lz->h_err != 0u) {
+        *lz->h_err = 0u;
+        LZ_CUDA(cudaMemsetAsync(lz->d_arrive, 0, 4 * sizeof(unsigned), lz->stream));
+        lz->last_error = "single-vector iteration: a grid barrier wait timed out";
+        return kErrCuda;
     }
     if (st != kOk) return st;
     // Y = V_{0..i} D_i
-    const int mfinal = (done_it + 1) * k;
-    st = upload(lz, lz->d_coef, D.data(), D.size());
-    if (st != kOk) return st;
     st = block_gemm(lz, mfinal, V, ldv, lz->d_coef, k, 0.0, d_y, ldy);
     if (st != kOk) return st;
     *iters_out = converged ? done_it : -1;

@@ -63,6 +63,23 @@ def test_oracle_lanczos_small_dense():
     assert itb > 0 and rel_err(S @ Z, Y) < 1e-8
 
 
+def test_oracle_block_of_one_is_single_vector_lanczos():
+    """A block of one column is the single-vector recurrence
+    (brwn_lanczos.cc:16-82 against :85-201 at k = 1): same stopping
+    iteration, same iterate to rounding -- the identity the GPU's
+    single-vector iteration relies on when it replaces the block QR by one
+    normalisation."""
+    g = golden("lanczos_N1000")
+    pos = g["pos"][:40]
+    M = so.dense_ewald_matrix(pos, np.ones(40), float(g["box"]), 1e-12)
+    z = np.random.default_rng(4).standard_normal(120)
+    for tol in (1e-5, 1e-8):
+        y, it = so.lanczos_sqrt(lambda x: M @ x, z, 100, tol)
+        Y, itb = so.block_lanczos_sqrt(lambda X: M @ X, z[:, None], 100, tol)
+        assert it > 0 and it == itb
+        assert rel_err(y, Y[:, 0]) < 1e-12
+
+
 def test_bspline_weights_partition_of_unity():
     for p in (4, 6, 8):
         for frac in (0.0, 0.25, 0.5, 0.999):

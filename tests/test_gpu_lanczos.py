@@ -89,7 +89,8 @@ def test_block_lanczos_vs_oracle_config1(gpu_available):
 def test_single_vector_vs_oracle_config1(gpu_available, reorth, fused, monkeypatch):
     """One RHS (the dot-product/axpy iteration, one normalisation per step;
     fused: one cooperative launch per iteration, else four launches) against
-    the FP64 oracle's Lanczos on the FP64 oracle SPME, config 1, tol 1e-6.
+    the FP64 oracle's single-vector Lanczos on the FP64 oracle SPME, config
+    1, tol 1e-6.
     With reorthogonalisation the basis stays orthonormal, so the iteration
     count matches the oracle's to within the checks issued ahead."""
     import stokesdt_b200 as sdt
@@ -111,9 +112,10 @@ def test_single_vector_vs_oracle_config1(gpu_available, reorth, fused, monkeypat
     assert its[0] + 1 <= lz.products() <= its[0] + 5
     o = so.SpmeOracle(g["rdi"], float(g["box"]), float(g["xi"]), float(g["rmax"]), 64, 6)
     o.update(g["pos"])
-    yo, ito = so.block_lanczos_sqrt(lambda X: o.mulvec(X.T).T, z.T, 100, 1e-6)
+    # the oracle's single-vector Lanczos (brwn_lanczos.cc:16-82)
+    yo, ito = so.lanczos_sqrt(lambda x: o.mulvec(x[None, :])[0], z[0], 100, 1e-6)
     assert ito > 0
-    assert rel_err(yo.T, y) < TOL
+    assert rel_err(yo[None, :], y) < TOL
     if reorth:
         assert abs(its[0] - ito) <= 2, (its, ito)
     # the same vector as the first column of a 2-RHS block agrees too

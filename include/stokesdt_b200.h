@@ -187,7 +187,10 @@ int sdt_lanczos_create(int dim, int max_iters, int max_nrhs, double tol, int dev
  * groups of max_nrhs like BrwnLanczos::Compute.  iters (optional, length
  * ceil(nrhs/max_nrhs)) receives the iteration count of each group, -1 if it
  * did not converge; the call then returns SDT_ERR_NOT_CONVERGED but y holds
- * the last iterate. */
+ * the last iterate.  A group of one vector is BrwnLanczos::Lanczos
+ * (src/brwn/brwn_lanczos.cc:16-82); its iterations run as one cooperative
+ * launch each, and a grid-barrier wait in it that runs out (about a second)
+ * makes the call return SDT_ERR_CUDA. */
 int sdt_lanczos_compute(sdt_lanczos *h, sdt_spme *mob, int nrhs, int ldz, const double *z,
                         int ldy, double *y, int *iters);
 

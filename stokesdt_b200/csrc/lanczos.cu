@@ -792,14 +792,17 @@ __device__ __forceinline__ double vec_warp_sum_parts(const double *part, int G)
 
 // part: [G] dot partials, [ma][G] reorthogonalisation partials (column-major,
 // so a column's partials are contiguous for the fold), [G] norm partials.
-// Wn as k_vec_scale.  dA/dB/dflag: the iteration's history slots (written
-// by CTA 0).  While the first barrier is pending, the CTA's rows of
+// W = V_i + ldv is the product's output, updated in place; it is passed as
+// its own pointer, never reached through the read-only V (whose loads may
+// take the non-coherent path).  Wn as k_vec_scale.  dA/dB/dflag: the
+// iteration's history slots (written by CTA 0).  While the first barrier is pending, the CTA's rows of
 // V_0 .. V_{i-1} are prefetched into L2 (the mobility product in between
 // has streamed far more than L2 holds), so the reorthogonalisation reads
 // them from there.
 __global__ void __launch_bounds__(kVecThreads, 1)
 k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__restrict__ V, int ldv,
-           double *__restrict__ Wn, double *__restrict__ part, unsigned *__restrict__ bars, int parity,
+           double *__restrict__ W, double *__restrict__ Wn, double *__restrict__ part, unsigned *__restrict__ bars,
+           int parity,
            unsigned skew, unsigned *__restrict__ err, double *__restrict__ dA, double *__restrict__ dB,
            double *__restrict__ dflag)
 {
@@ -811,7 +814,6 @@ k_vec_iter(int n, int rows, int nchunks, int ma, int reorth, const double *__res
     unsigned *bar = bars + parity;
     if (blockIdx.x == 0 && tid == 0) bars[parity ^ 1] = 0u;
     const double *Vi = V + (size_t)(ma - 1) * ldv;
-    double *W = const_cast<double *>(Vi) + ldv;
     double *p1 = part, *p2 = part + G, *p3 = p2 + (size_t)G * ma;
     // after a wait that ran out: the iteration reads as a breakdown, so the
     // host stops issuing, and the flag in *err reports it
@@ -1303,8 +1305,8 @@ static int vec_iteration(LanczosState *lz, int it, double *V, double *Wn, double
         double *part = lz->d_part;
         unsigned *bars = lz->d_arrive + 1, *err = lz->d_arrive + 3;
         void *args[] = {(void *)&n, (void *)&rows, (void *)&nchunks, (void *)&ma, (void *)&rev, (void *)&V,
-                        (void *)&ldv, (void *)&Wn, (void *)&part, (void *)&bars, (void *)&parity, (void *)&skew,
-                        (void *)&err, (void *)&dA, (void *)&dB, (void *)&dflag};
+                        (void *)&ldv, (void *)&W, (void *)&Wn, (void *)&part, (void *)&bars, (void *)&parity,
+                        (void *)&skew, (void *)&err, (void *)&dA, (void *)&dB, (void *)&dflag};
         pt.begin(1);
         const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_vec_iter, dim3(lz->vec_grid),
                                                           dim3(kVecThreads), args, 0, lz->stream);

@@ -114,9 +114,10 @@ k_reduce_parts(int nparts, int count, const double *__restrict__ part, double *_
 
 // Out[b][e] = beta * Out[b][e] + alpha * sum_{a < ma} A[a][e] * C[a][b], b < mb <= 32.
 // One thread per row e; every thread reads its A values before writing, so
-// A == Out (in-place right multiplication) is allowed.
+// A == Out (in-place right multiplication) is allowed (hence no __restrict__
+// on A).
 __global__ void __launch_bounds__(256)
-k_block_gemm(int n, int ma, const double *__restrict__ A, int lda, const double *__restrict__ C,
+k_block_gemm(int n, int ma, const double *A, int lda, const double *__restrict__ C,
              int mb, double alpha, double beta, double *Out, int ldo)
 {
     extern __shared__ double sc[];  // [ma][mb]
